@@ -1,0 +1,307 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 GDF P2 MHD step: P2 MHD cell-updates/s.
+
+Workload: the MHD rotor at 512x512, P2 modal DG in FP64, HLLD flux, KXRCF
+detector + characteristic TVB limiter + positivity limiter, SSP-RK3 (the
+plain method at scale). One step = one full SSP-RK3 step of the whole
+grid (3 stages + limiters + div-free reconstruction + dt); one
+cell-update = one cell advanced by one step.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs one process per GPU under torchrun; each rank advances its own
+replica of the workload (the path runs on one GPU; replicas only), timed
+on the device and reported as the max over ranks. Prints one JSON line on
+rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "freljord-cfd-arsenal_b200"))
+
+METRIC = "P2 MHD cell-updates/s on 1 B200, learned-indicator vs plain at equal L1 err"
+UNIT = "cell-updates/s"
+NX = NY = 512
+WORKLOAD = ("MHD rotor 512x512 on [0,1]^2, P2 modal DG FP64 (8 vars x 10 modal slots), HLLD flux, "
+            "KXRCF detector + characteristic TVB (M=10) + positivity limiter, corner-Ez CT + Balsara "
+            "div-free B, SSP-RK3, CFL 0.15 (plain method)")
+
+# Compulsory HBM bytes per cell for one launch of each kernel kind (FP64,
+# 52 live modal slots = 416 B per cell state). See DESIGN.md "roofline".
+ALG_BYTES_PER_CELL = {
+    "face_x": 416 + 40 * 8 + 5 * 8,          # cell modes once, Fxhat + EzRL of the cell's face
+    "face_y": 416 + 40 * 8 + 5 * 8,
+    "vertex": 416 + 8,                       # cell modes once, one vertex Ez
+    "cell": (1888 + 2 * 2304) / 3,           # U + faces' Fhat + U0/UI read, UI (+U0) written; stage mean
+    "bface": 2 * (5 * 8 + 8 + 3 * 8 * 3),    # two faces: Ez points, vertex, B/B0/BI read+written
+    "limit": 416 + 2 * 6 * 8 + 416 + 4,      # pre-limit modes, 4 face polys (2 owned), limited modes, flag
+    "set_bc": 0.0,
+    "dt": 8 * 8,                             # cell averages
+}
+
+
+def read_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+        self.t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict | None:
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.t:
+            self.t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names[1:], f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def make_state(gdf):
+    cfg, _ = gdf.problem_config(gdf.PROB_ROTOR, NX, NY)
+    uh, bx, by = gdf.init_data(cfg, gdf.PROB_ROTOR)
+    return cfg, uh, bx, by
+
+
+def cpu_baseline(gdf, steps: int):
+    """The oracle (CPU restatement of the reference) on the same workload."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    from oracle import Oracle, set_threads
+    cores = set_threads(0)
+    cfg, uh, bx, by = make_state(gdf)
+    o = Oracle(cfg)
+    o.prepare(uh, bx, by)
+    t, _, _ = o.step(uh, bx, by, 0.0, 1e9)          # warm-up step
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        t, _, _ = o.step(uh, bx, by, t, 1e9)
+    el = time.perf_counter() - t0
+    return {"value": NX * NY * steps / el, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"rotor {NX}x{NY} (the benchmark workload), {steps} timed steps after prepare and 1 "
+                      f"warm-up step, oracle/gdf_oracle.cpp with OpenMP on {cores} host threads",
+            "seconds": el}
+
+
+def run_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    import gdf
+    k = max(1, min(args.steps, 10))
+    w = max(0, min(args.warmup, 1))
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    from oracle import Oracle, set_threads
+    cores = set_threads(0)
+    cfg, uh, bx, by = make_state(gdf)
+    o = Oracle(cfg)
+    o.prepare(uh, bx, by)
+    t = 0.0
+    for _ in range(w):
+        t, _, _ = o.step(uh, bx, by, t, 1e9)
+    t0 = time.perf_counter()
+    for _ in range(k):
+        t, _, _ = o.step(uh, bx, by, t, 1e9)
+    el = time.perf_counter() - t0
+    value = NX * NY * k / el
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": el / k * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "grid": [NX, NY], "problem": "rotor"},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{k} steps (of --steps {args.steps}) of the rotor {NX}x{NY} after prepare "
+                                   f"and {w} warm-up step(s); the reference Fortran cannot be built here "
+                                   "(no Fortran compiler), so its CPU restatement oracle/gdf_oracle.cpp runs"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    world, rank, local = dist_env()
+    import numpy as np
+    import gdf
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    gdf.set_device(local)
+    cfg, uh, bx, by = make_state(gdf)
+    s = gdf.Solver(cfg)
+    s.upload(uh, bx, by)
+    s.prepare()
+    s.advance_timed(1e9, max(3, args.warmup))       # warm-up (also captures the step graph)
+    if dist:
+        dist.barrier()
+    clk = ClockSampler(local)
+    clk.start()
+    time.sleep(0.3)
+    l0 = s.kernel_launches()
+    _, taken, ms = s.advance_timed(1e9, args.steps)
+    launches = s.kernel_launches() - l0
+    clocks = clk.stop()
+    ms_max = ms
+    if dist:
+        import torch
+        tt = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms_max = float(tt.item())
+    value = world * NX * NY * args.steps / (ms_max / 1e3)
+
+    # per-kernel timing (events around every launch) for the roofline
+    prof = s.profile(2)
+    dom = max((k for k in prof if k in ALG_BYTES_PER_CELL), key=lambda k: prof[k][0] * prof[k][1])
+    dom_ms, dom_per_step = prof[dom]
+    alg_bytes = ALG_BYTES_PER_CELL[dom] * NX * NY
+    peak, peak_kind = read_peaks()
+    achieved = alg_bytes / (dom_ms / 1e3) / 1e9
+    traffic = None
+    tp = os.path.join(REPO, "profiles", "traffic_rotor512.json")
+    if os.path.exists(tp):
+        try:
+            traffic = json.load(open(tp)).get(dom)
+        except Exception:
+            traffic = None
+
+    # end to end through the public API with host buffers (pinned)
+    import torch
+    pin = lambda a: torch.from_numpy(a).pin_memory().numpy()   # noqa: E731
+    huh, hbx, hby = pin(uh), pin(bx), pin(by)
+    s.upload(huh, hbx, hby)
+    s.prepare()
+    huh2, hbx2, hby2 = s.download()
+    huh, hbx, hby = pin(huh2), pin(hbx2), pin(hby2)
+    e2e_steps = max(2, min(args.steps, 10))
+    t = 0.0
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        s.upload(huh, hbx, hby)
+        s.t = t
+        t, _, _ = s.step(1e9, flags=False)
+        s.download_into(huh, hbx, hby)
+    e2e_el = time.perf_counter() - t0
+    e2e = world * NX * NY * e2e_steps / e2e_el
+    io_bytes = huh.nbytes + hbx.nbytes + hby.nbytes
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(gdf, args.cpu_steps)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "grid": [NX, NY], "problem": "rotor", "method": "plain",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": "inputs larger than L2 (uh alone is 168 MB per copy; 126 MB L2)",
+                       "timing": "CUDA events on the library stream around graph replays"},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "alg_bytes_per_launch": alg_bytes, "ms_per_launch": dom_ms,
+                         "launches_per_step": dom_per_step},
+            "kernels_ms_per_launch": {k: v[0] for k, v in prof.items() if v[1]},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(io_bytes),
+                    "d2h_bytes_per_step": int(io_bytes), "steps": e2e_steps},
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "steps_taken": taken,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    s.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

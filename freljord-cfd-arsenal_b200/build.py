@@ -1,0 +1,79 @@
+"""Build the sm_100a shared libraries of the GDF P2 step, in-tree.
+
+Produces, under freljord-cfd-arsenal_b200/lib/:
+  libgdf_b200.so        the product build (FMA contraction on)
+  libgdf_b200_exact.so  the same sources with --fmad=false, whose arithmetic
+                        follows an FMA-free CPU build of the reference
+Both export the C ABI of include/gdf.h. Rebuilds only what is out of date.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+LIB = os.path.join(PKG, "lib")
+BUILD = os.path.join(PKG, "_build")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+HOST_CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
+
+KERNEL_SRC = os.path.join(CSRC, "gdf_kernels.cu")
+HOST_SRC = os.path.join(CSRC, "gdf_host.cpp")
+HEADERS = [os.path.join(CSRC, f) for f in ("gdf_physics.cuh", "gdf_kernels.cuh")] + [
+    os.path.join(REPO, "include", "gdf.h")]
+
+
+def _nvcc() -> str:
+    for cand in (shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found: the CUDA toolkit is required to build the library")
+
+
+def _stale(target: str, deps: list[str]) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def _run(cmd: list[str]) -> None:
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("build failed: " + " ".join(cmd[:3]) + " ...")
+
+
+def build(verbose: bool = False) -> dict:
+    os.makedirs(LIB, exist_ok=True)
+    os.makedirs(BUILD, exist_ok=True)
+    nvcc = _nvcc()
+    host_o = os.path.join(BUILD, "gdf_host.o")
+    if _stale(host_o, [HOST_SRC] + HEADERS):
+        _run([HOST_CXX, "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-march=x86-64",
+              "-c", HOST_SRC, "-o", host_o])
+    out = {}
+    for name, flags in (("libgdf_b200.so", ["--fmad=true"]),
+                        ("libgdf_b200_exact.so", ["--fmad=false", "-DGDF_EXACT=1"])):
+        obj = os.path.join(BUILD, name.replace(".so", ".o"))
+        so = os.path.join(LIB, name)
+        if _stale(obj, [KERNEL_SRC] + HEADERS):
+            cmd = [nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17", *flags,
+                   "-Xcompiler", "-fPIC,-ffp-contract=off", "-c", KERNEL_SRC, "-o", obj]
+            if verbose:
+                cmd.insert(1, "-Xptxas=-v")
+            _run(cmd)
+        if _stale(so, [obj, host_o]):
+            _run([nvcc, *ARCH, "-shared", "-o", so, obj, host_o])
+        out[name] = so
+    return out
+
+
+if __name__ == "__main__":
+    for k, v in build(verbose="-v" in sys.argv).items():
+        print(k, "->", v)

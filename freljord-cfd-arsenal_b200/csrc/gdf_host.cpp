@@ -1,0 +1,301 @@
+// gdf_host.cpp -- host side of the C ABI that needs no device: the
+// configuration presets and the initial data (the reference's L1 set-up,
+// init_data.f90 with the init*.txt problem includes). Compiled without FMA
+// contraction so the projections round exactly as the reference's loops.
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "../../include/gdf.h"
+
+namespace {
+
+constexpr int NG = 5, NP = 10, NE = 8;
+
+const double kLam[NG] = {-0.9061798459386639927976269, -0.5384693101056830910363144, 0,
+                         0.5384693101056830910363144, 0.9061798459386639927976269};
+const double kW[NG] = {0.2369268850561890875142640, 0.4786286704993664680412915, 0.5688888888888888888888889,
+                       0.4786286704993664680412915, 0.2369268850561890875142640};
+
+// Point values of the eight conserved variables of a problem.
+struct Init {
+  int problem;
+  double g;
+  double prm[8];
+
+  void primitive(double x, double y, double& rho, double& v1, double& v2, double& v3, double& p, double& B1,
+                 double& B2, double& B3) const {
+    const double pi = 4 * std::atan(1.0);
+    rho = v1 = v2 = v3 = p = B1 = B2 = B3 = 0;
+    switch (problem) {
+      case GDF_PROB_VORTEX: {  // init1.txt:3-20
+        const double r2 = x * x + y * y;
+        const double e = std::exp(0.5 * (1 - r2));
+        p = 1 - r2 / (8.0 * (pi * pi)) * std::exp(1 - r2);
+        rho = 1;
+        v1 = 1 - 1.0 / (2.0 * pi) * y * e;
+        v2 = 1 + 1.0 / (2.0 * pi) * x * e;
+        B1 = -1.0 / (2.0 * pi) * y * e;
+        B2 = 1.0 / (2.0 * pi) * x * e;
+        break;
+      }
+      case GDF_PROB_ORSZAG_TANG:  // init3.txt:3-16
+        p = g;
+        rho = g * g;
+        v1 = -std::sin(y);
+        v2 = std::sin(x);
+        B1 = -std::sin(y);
+        B2 = std::sin(2.0 * x);
+        break;
+      case GDF_PROB_ROTOR: {  // taper shape of Rotor_functions.f90, rim speed prm[5]
+        const double cx = prm[0], cy = prm[1], r0 = prm[2], r1 = prm[3], rin = prm[4], u0 = prm[5];
+        const double r = std::sqrt((x - cx) * (x - cx) + (y - cy) * (y - cy));
+        const double f = (r1 - r) / (r1 - r0);
+        if (r < r0) {
+          rho = rin;
+          v1 = -u0 * (y - cy) / r0;
+          v2 = u0 * (x - cx) / r0;
+        } else if (r < r1) {
+          rho = 1.0 + (rin - 1.0) * f;
+          v1 = -f * u0 * (y - cy) / r;
+          v2 = f * u0 * (x - cx) / r;
+        } else {
+          rho = 1.0;
+        }
+        p = prm[6];
+        B1 = prm[7];
+        break;
+      }
+      case GDF_PROB_BLAST: {  // p0.f90 shape about (prm[0], prm[1])
+        const double dx = x - prm[0], dy = y - prm[1];
+        const double r = std::sqrt(dx * dx + dy * dy);
+        p = (r <= prm[2]) ? prm[3] : prm[4];
+        rho = prm[5];
+        B1 = prm[6];
+        B2 = prm[7];
+        break;
+      }
+      default: {  // Cloud_Shock_functions.f90
+        const double r = std::sqrt((x - 1.4) * (x - 1.4) + (y - 0.5) * (y - 0.5));
+        if (x <= 1.2) {
+          rho = 3.88968; v3 = -0.05234; p = 14.2641; B1 = 1; B3 = 3.9353;
+        } else {
+          rho = (r >= 0.18) ? 1.0 : 5.0; v1 = -3.3156; p = 0.04; B1 = 1; B3 = 1;
+        }
+        break;
+      }
+    }
+  }
+
+  void conserved(double x, double y, double* U) const {
+    double rho, v1, v2, v3, p, B1, B2, B3;
+    primitive(x, y, rho, v1, v2, v3, p, B1, B2, B3);
+    const double g1 = g - 1;
+    U[0] = rho;
+    U[1] = rho * v1;
+    U[2] = rho * v2;
+    U[3] = rho * v3;
+    // U5 of the init*.txt includes: only init6 carries the third components
+    if (problem == GDF_PROB_CLOUD_SHOCK)
+      U[4] = p / g1 + 0.5 * rho * (v1 * v1 + v2 * v2 + v3 * v3) + 0.5 * (B1 * B1 + B2 * B2 + B3 * B3);
+    else
+      U[4] = p / g1 + 0.5 * rho * (v1 * v1 + v2 * v2) + 0.5 * (B1 * B1 + B2 * B2);
+    U[5] = B1;
+    U[6] = B2;
+    U[7] = B3;
+  }
+};
+
+void default_params(int problem, double* prm) {
+  const double pi = 4 * std::atan(1.0);
+  for (int q = 0; q < 8; ++q) prm[q] = 0;
+  if (problem == GDF_PROB_ROTOR) {
+    // centre, r0, r1, inner density, rim speed (angular speed 20 at r0 = 0.1),
+    // pressure, Bx
+    const double v[8] = {0.5, 0.5, 0.1, 0.115, 10.0, 2.0, 1.0, 5.0 / std::sqrt(4 * pi)};
+    std::memcpy(prm, v, sizeof(v));
+  } else if (problem == GDF_PROB_BLAST) {
+    const double v[8] = {0, 0, 0.1, 1000, 0.1, 1.0, 100.0 / std::sqrt(8 * pi), 100.0 / std::sqrt(8 * pi)};
+    std::memcpy(prm, v, sizeof(v));
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int gdf_config_reference(int32_t nx, int32_t ny, GdfConfig* out) {
+  if (!out || nx < 2 || ny < 2) return GDF_ERR_ARG;
+  std::memset(out, 0, sizeof(*out));
+  out->nx = nx;
+  out->ny = ny;
+  out->xa = 0; out->xb = 1; out->ya = 0; out->yb = 1;
+  out->bc_r = out->bc_l = out->bc_u = out->bc_d = GDF_BC_PERIODIC;
+  out->gamma = 5.0 / 3.0;        // com.txt:7
+  out->gamma_flux = 5.0 / 3.0;   // MHD_flux.f90:7, eigenmatrix.f90:19
+  out->flux_type = GDF_FLUX_HLL; // com.txt:1
+  out->cfl = 0.15;               // calculate_dt.f90:8
+  out->tvb_m = 10.0;             // init6.txt M
+  out->tvb_slope = 0.75;         // TVB_Limiter_P2.f90:111
+  out->hlld_eps = 1e-4;          // HLLD_Flux.f90:126
+  out->pp_limiter = 0;
+  out->faceb_limiter = 0;
+  out->ez_face_fhat = 0;
+  out->eig_p_typo = 0;
+  out->eig_identity = 1;
+  out->eig_y_zero_w = 0;
+  out->kml_w_term = 1;
+  out->dt_floor_stop = 1;
+  out->umax_all_vars = 0;
+  out->detector = GDF_DETECT_ALL;
+  out->kxrcf_ck = 0.0;           // KXRCF_Detector.f90:7
+  out->kxrcf_sticky = 1;
+  return GDF_OK;
+}
+
+int gdf_problem_config(int32_t problem, int32_t nx, int32_t ny, GdfConfig* out, double* tend) {
+  int rc = gdf_config_reference(nx, ny, out);
+  if (rc) return rc;
+  const double pi = 4 * std::atan(1.0);
+  double te = 0;
+  switch (problem) {
+    case GDF_PROB_VORTEX:
+      out->xa = -10; out->xb = 10; out->ya = -10; out->yb = 10;
+      out->tvb_m = 1000000.0;
+      te = 0;
+      break;
+    case GDF_PROB_ORSZAG_TANG:
+      out->xa = 0; out->xb = 2 * pi; out->ya = 0; out->yb = 2 * pi;
+      out->tvb_m = 50.0;
+      te = 0.5;
+      break;
+    case GDF_PROB_ROTOR:
+      out->gamma = 1.4;
+      out->flux_type = GDF_FLUX_HLLD;
+      out->pp_limiter = 1;
+      out->detector = GDF_DETECT_KXRCF;
+      out->kxrcf_ck = 1.0;
+      te = 0.295;
+      break;
+    case GDF_PROB_BLAST:
+      out->xa = -0.5; out->xb = 0.5; out->ya = -0.5; out->yb = 0.5;
+      out->bc_r = out->bc_l = out->bc_u = out->bc_d = GDF_BC_OUTFLOW;
+      out->gamma = 1.4;
+      out->flux_type = GDF_FLUX_HLLD;
+      out->pp_limiter = 1;
+      out->detector = GDF_DETECT_KXRCF;
+      out->kxrcf_ck = 1.0;
+      te = 0.01;
+      break;
+    case GDF_PROB_CLOUD_SHOCK:
+      out->xa = 0; out->xb = 2; out->ya = 0; out->yb = 1;
+      out->bc_r = out->bc_l = out->bc_u = out->bc_d = GDF_BC_OUTFLOW;
+      te = 0.6;
+      break;
+    default:
+      return GDF_ERR_ARG;
+  }
+  if (tend) *tend = te;
+  return GDF_OK;
+}
+
+// init_data.f90:21-121
+int gdf_init_data(const GdfConfig* cfg, int32_t problem, const double* params, double* uh, double* bx,
+                  double* by) {
+  if (!cfg || !uh || !bx || !by || problem < 0 || problem > 4) return GDF_ERR_ARG;
+  const int Nx = cfg->nx, Ny = cfg->ny;
+  Init P;
+  P.problem = problem;
+  P.g = cfg->gamma;
+  default_params(problem, P.prm);
+  if (params) std::memcpy(P.prm, params, sizeof(P.prm));
+  const bool shock = (problem == GDF_PROB_BLAST || problem == GDF_PROB_CLOUD_SHOCK);
+  const double hx = (cfg->xb - cfg->xa) / Nx, hy = (cfg->yb - cfg->ya) / Ny;
+  const double hx1 = 0.5 * hx, hy1 = 0.5 * hy;
+  const size_t NX2 = (size_t)Nx + 2, NY2 = (size_t)Ny + 2, plane = NX2 * NY2;
+  std::memset(uh, 0, plane * NP * NE * sizeof(double));
+  std::memset(bx, 0, (size_t)(Nx + 1) * Ny * 3 * sizeof(double));
+  std::memset(by, 0, (size_t)Nx * (Ny + 1) * 3 * sizeof(double));
+  auto U = [&](int i, int j, int d, int n) -> double& { return uh[i + NX2 * (j + NY2 * (d + 10 * n))]; };
+  std::vector<double> Xc(Nx + 1), Yc(Ny + 1);
+  for (int i = 1; i <= Nx; ++i) Xc[i] = cfg->xa + (i - 0.5) * hx;
+  for (int j = 1; j <= Ny; ++j) Yc[j] = cfg->ya + (j - 0.5) * hy;
+  // values of the basis at the 5x5 Gauss points (get_basis.f90 phiG)
+  const double c13 = 1.0 / 3.0;
+  auto phiG = [&](int a, int b, int d) {
+    const double li = kLam[a], lj = kLam[b];
+    switch (d) {
+      case 0: return 1.0;
+      case 1: return li;
+      case 2: return lj;
+      case 3: return li * li - c13;
+      case 4: return li * lj;
+      default: return lj * lj - c13;
+    }
+  };
+  const double mm[6] = {1, 1.0 / 3.0, 1.0 / 3.0, 4.0 / 45.0, 1.0 / 9.0, 4.0 / 45.0};
+  const double mmE[3] = {1, 1.0 / 3.0, 4.0 / 45.0};
+  double Uv[NE];
+  if (!shock) {
+    for (int i = 1; i <= Nx; ++i)
+      for (int j = 1; j <= Ny; ++j) {
+        // init_data.f90:37-63: only modes 1..6 pass the projection mask
+        double acc[6][NE];
+        for (int d = 0; d < 6; ++d)
+          for (int n = 0; n < NE; ++n) acc[d][n] = 0.0;
+        for (int d = 0; d < 6; ++d)
+          for (int a = 0; a < NG; ++a)
+            for (int b = 0; b < NG; ++b) {
+              P.conserved(Xc[i] + hx1 * kLam[a], Yc[j] + hy1 * kLam[b], Uv);
+              const double f = kW[a] * kW[b] * phiG(a, b, d);
+              for (int n = 0; n < NE; ++n) acc[d][n] = acc[d][n] + f * Uv[n];
+            }
+        for (int d = 0; d < 6; ++d)
+          for (int n = 0; n < NE; ++n) U(i, j, d, n) = 0.25 * acc[d][n] / mm[d];
+      }
+    // face projections of Bx and By (init_data.f90:65-90)
+    for (int i = 0; i <= Nx; ++i)
+      for (int j = 1; j <= Ny; ++j)
+        for (int d = 0; d < 3; ++d) {
+          double acc = 0.0;
+          for (int b = 0; b < NG; ++b) {
+            P.conserved(cfg->xa + i * hx, Yc[j] + hy1 * kLam[b], Uv);
+            const double e = d == 0 ? 1.0 : d == 1 ? kLam[b] : kLam[b] * kLam[b] - c13;
+            acc = acc + 0.5 * kW[b] * e * Uv[5];
+          }
+          bx[i + (size_t)(Nx + 1) * ((j - 1) + (size_t)Ny * d)] = acc / mmE[d];
+        }
+    for (int i = 1; i <= Nx; ++i)
+      for (int j = 0; j <= Ny; ++j)
+        for (int d = 0; d < 3; ++d) {
+          double acc = 0.0;
+          for (int a = 0; a < NG; ++a) {
+            P.conserved(Xc[i] + hx1 * kLam[a], cfg->ya + j * hy, Uv);
+            const double e = d == 0 ? 1.0 : d == 1 ? kLam[a] : kLam[a] * kLam[a] - c13;
+            acc = acc + 0.5 * kW[a] * e * Uv[6];
+          }
+          by[(i - 1) + (size_t)Nx * (j + (size_t)(Ny + 1) * d)] = acc / mmE[d];
+        }
+  } else {
+    // shock == 1 (init_data.f90:92-121): point values, higher modes zero
+    for (int i = 1; i <= Nx; ++i)
+      for (int j = 1; j <= Ny; ++j) {
+        P.conserved(Xc[i], Yc[j], Uv);
+        for (int n = 0; n < NE; ++n) U(i, j, 0, n) = Uv[n];
+      }
+    for (int i = 0; i <= Nx; ++i)
+      for (int j = 1; j <= Ny; ++j) {
+        P.conserved(cfg->xa + i * hx, Yc[j], Uv);
+        bx[i + (size_t)(Nx + 1) * (j - 1)] = Uv[5];
+      }
+    for (int i = 1; i <= Nx; ++i)
+      for (int j = 0; j <= Ny; ++j) {
+        P.conserved(Xc[i], cfg->ya + j * hy, Uv);
+        by[(i - 1) + (size_t)Nx * j] = Uv[6];
+      }
+  }
+  return GDF_OK;
+}
+
+}  // extern "C"

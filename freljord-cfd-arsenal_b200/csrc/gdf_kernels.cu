@@ -1,0 +1,1627 @@
+// gdf_kernels.cu -- sm_100a kernels of the GDF P2 step and the C ABI of
+// include/gdf.h.
+//
+// One SSP-RK3 step (RK3.f90:60-151) is:
+//   k_dt_partial + k_dt_final                 calculate_dt + t update
+//   3 x [ k_set_bc                            set_bc (stage 1 only; the
+//                                             other stages reuse the one
+//                                             that ends the previous stage)
+//         k_face<0>, k_face<1>                Lh traces + Riemann (Fxhat,
+//                                             Fyhat) + LhEz face Ez
+//         k_vertex                            LhEz vertex Ez (2-D solvers)
+//         k_cell                              Lh volume + surface integral,
+//                                             fused with the RK combine
+//         k_bface                             LhEz dEz + face-B combine
+//         k_limit                             TVB_Limiter_P2 (+KXRCF, +pp)
+//                                             fused with div_free_Balsara
+//         k_set_bc ]
+// Every kernel is one thread per item (face point, vertex, cell, face) and
+// computes that item sequentially in the reference's order, so a build with
+// --fmad=false reproduces the reference arithmetic value for value.
+// All device waits are stream-ordered; no kernel spins.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/gdf.h"
+#include "gdf_kernels.cuh"
+
+#ifndef GDF_EXACT
+#define GDF_EXACT 0
+#endif
+
+namespace gdf {
+
+// ------------------------------------------------------------ live slots --
+__host__ __device__ constexpr int LI(int n, int d) {
+  return n < 5 ? n * 6 + d
+               : n == 5 ? 30 + (d <= 6 ? d : 7)
+                        : n == 6 ? 38 + (d <= 5 ? d : (d == 7 ? 6 : 7)) : 46 + d;
+}
+__constant__ unsigned char c_live_n[NLIVE] = {0, 0, 0, 0, 0, 0, 1, 1, 1, 1, 1, 1, 2, 2, 2, 2, 2, 2,
+                                              3, 3, 3, 3, 3, 3, 4, 4, 4, 4, 4, 4, 5, 5, 5, 5, 5, 5,
+                                              5, 5, 6, 6, 6, 6, 6, 6, 6, 6, 7, 7, 7, 7, 7, 7};
+__constant__ unsigned char c_live_d[NLIVE] = {0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5,
+                                              0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5,
+                                              6, 8, 0, 1, 2, 3, 4, 5, 7, 9, 0, 1, 2, 3, 4, 5};
+
+__device__ __forceinline__ long long gtid() { return (long long)blockIdx.x * blockDim.x + threadIdx.x; }
+
+// ------------------------------------------------------------- set_bc ----
+// set_bc.f90:5-27. Ghost (i,j) takes the value of (mapx(i), mapy(j)): the
+// x pass first and then the y pass over full rows make every corner ghost
+// the image of an interior cell under both maps. zeroB also clears the
+// ghost Bx/By modes, as div_free_Balsara.f90:11 leaves them.
+__global__ void k_set_bc(const __grid_constant__ Consts K, double* __restrict__ U, int zeroB,
+                         const Scal* __restrict__ sc) {
+  if (sc && !sc->active) return;
+  const long long nper = 2LL * (K.nx + 2) + 2LL * K.ny;
+  const long long t = gtid();
+  if (t >= nper * NLIVE) return;
+  const int k = (int)(t / nper);
+  const long long q = t - (long long)k * nper;
+  int i, j;
+  if (q < K.nx + 2) { i = (int)q; j = 0; }
+  else if (q < 2LL * (K.nx + 2)) { i = (int)(q - (K.nx + 2)); j = K.ny + 1; }
+  else if (q < 2LL * (K.nx + 2) + K.ny) { i = 0; j = (int)(q - 2LL * (K.nx + 2)) + 1; }
+  else { i = K.nx + 1; j = (int)(q - 2LL * (K.nx + 2) - K.ny) + 1; }
+  int si = i, sj = j;
+  if (i == 0) si = (K.bc_l == GDF_BC_PERIODIC) ? K.nx : 1;
+  else if (i == K.nx + 1) si = (K.bc_r == GDF_BC_PERIODIC) ? 1 : K.nx;
+  if (j == 0) sj = (K.bc_d == GDF_BC_PERIODIC) ? K.ny : 1;
+  else if (j == K.ny + 1) sj = (K.bc_u == GDF_BC_PERIODIC) ? 1 : K.ny;
+  const int n = c_live_n[k], d = c_live_d[k];
+  const long long off = K.plane * (d + 10 * n);
+  double v = U[off + si + (long long)K.nx2 * sj];
+  if (zeroB && (n == 5 || n == 6)) v = 0.0;
+  U[off + i + (long long)K.nx2 * j] = v;
+}
+
+// ---------------------------------------------------- face Riemann -------
+// Lh.f90:72-265 and LhEz.f90:6-31 for one face quadrature point.
+// DIR 0: x face (i = 0..Nx, j = 1..Ny) between cells (i,j) and (i+1,j).
+// DIR 1: y face (i = 1..Nx, j = 0..Ny) between cells (i,j) and (i,j+1).
+template <int DIR>
+__global__ void __launch_bounds__(128) k_face(const __grid_constant__ Consts K, const double* __restrict__ U,
+                                              double* __restrict__ Fh_out, double* __restrict__ Ez_out,
+                                              const Scal* __restrict__ sc) {
+  if (sc && !sc->active) return;
+  const int nf = DIR == 0 ? K.nx + 1 : K.nx;
+  const int nr = DIR == 0 ? K.ny : K.ny + 1;
+  const long long item = gtid();
+  if (item >= (long long)nf * NG * nr) return;
+  const int i0 = (int)(item % nf);
+  const long long r = item / nf;
+  const int g = (int)(r % NG);
+  const int j0 = (int)(r / NG);
+  long long cL, cR;
+  if (DIR == 0) {
+    cL = i0 + (long long)K.nx2 * (j0 + 1);
+    cR = cL + 1;
+  } else {
+    cL = (i0 + 1) + (long long)K.nx2 * j0;
+    cR = cL + K.nx2;
+  }
+  double uL[NE], uR[NE];
+#pragma unroll
+  for (int n = 0; n < NE; ++n) {
+    double a = 0.0, b = 0.0;
+#pragma unroll
+    for (int d = 0; d < NP; ++d) {
+      if (!live_mode(n, d)) continue;
+      const long long off = K.plane * (d + 10 * n);
+      const double pl = DIR == 0 ? K.phiGR[g][d] : K.phiGU[g][d];
+      const double pr = DIR == 0 ? K.phiGL[g][d] : K.phiGD[g][d];
+      a = a + U[off + cL] * pl;
+      b = b + U[off + cR] * pr;
+    }
+    uL[n] = a;
+    uR[n] = b;
+  }
+  double Fh[NE], fL[NE], fR[NE];
+  face_flux(K.P, uL, uR, DIR, Fh, fL, fR);
+  const long long fp = DIR == 0 ? K.fxplane : K.fyplane;
+  const long long o = i0 + (long long)nf * j0;
+#pragma unroll
+  for (int n = 0; n < NE; ++n) Fh_out[(n * NG + g) * fp + o] = Fh[n];
+  double ez;
+  if (DIR == 0) {
+    if (K.ez_fhat) {
+      ez = -Fh[6];
+    } else {
+      const double S = fmax2(fabs(uL[1] / uL[0]), fabs(uR[1] / uR[0]));
+      ez = -0.5 * (fL[6] + fR[6] - S * (uR[6] - uL[6]));
+    }
+  } else {
+    if (K.ez_fhat) {
+      ez = Fh[5];
+    } else {
+      const double S = fmax2(fabs(uL[2] / uL[0]), fabs(uR[2] / uR[0]));
+      ez = 0.5 * (fL[5] + fR[5] - S * (uR[5] - uL[5]));
+    }
+  }
+  Ez_out[g * fp + o] = ez;
+}
+
+// ------------------------------------------------------- vertex Ez -------
+// LhEz.f90:34-69: corner traces of the four cells around vertex (i,j),
+// i = 0..Nx, j = 0..Ny, and the 2-D Riemann solver.
+__global__ void __launch_bounds__(128) k_vertex(const __grid_constant__ Consts K, const double* __restrict__ U,
+                                                double* __restrict__ EzV, const Scal* __restrict__ sc) {
+  if (sc && !sc->active) return;
+  const long long item = gtid();
+  if (item >= K.vplane) return;
+  const int i = (int)(item % (K.nx + 1));
+  const int j = (int)(item / (K.nx + 1));
+  const long long cLD = i + (long long)K.nx2 * j;  // cell (i,j): its RU corner
+  const long long cRD = cLD + 1;                   // (i+1,j): LU corner
+  const long long cLU = cLD + K.nx2;               // (i,j+1): RD corner
+  const long long cRU = cLU + 1;                   // (i+1,j+1): LD corner
+  double URU[NE], ULU[NE], URD[NE], ULD[NE];
+#pragma unroll
+  for (int n = 0; n < NE; ++n) {
+    double a = 0, b = 0, c = 0, e = 0;
+#pragma unroll
+    for (int d = 0; d < NP; ++d) {
+      if (!live_mode(n, d)) continue;
+      const long long off = K.plane * (d + 10 * n);
+      a = a + U[off + cRU] * K.phiLD[d];
+      b = b + U[off + cLU] * K.phiRD[d];
+      c = c + U[off + cRD] * K.phiLU[d];
+      e = e + U[off + cLD] * K.phiRU[d];
+    }
+    URU[n] = a; ULU[n] = b; URD[n] = c; ULD[n] = e;
+  }
+  EzV[item] = vertex_ez(K.P, URU, ULU, URD, ULD);
+}
+
+// ------------------------------------------------ residual + combine -----
+// Lh.f90:11-68 (volume), :268-304 (surface, mass) and the RK3.f90 stage
+// combine for one cell of the whole (Nx+2)x(Ny+2) array (ghost cells have
+// du = 0, as Lh leaves them). stage 0 writes du instead (gdf_lh).
+constexpr int CELL_BS = 64;
+
+__global__ void __launch_bounds__(CELL_BS) k_cell(const __grid_constant__ Consts K, const double* __restrict__ U,
+                                                  double* __restrict__ U0, double* __restrict__ UI,
+                                                  const double* __restrict__ Fxh, const double* __restrict__ Fyh,
+                                                  double* __restrict__ duout, const Scal* __restrict__ sc, int stage) {
+  __shared__ double ms[NLIVE * CELL_BS];
+  if (sc && !sc->active) return;
+  const long long item = gtid();
+  if (item >= K.plane) return;
+  const int tid = threadIdx.x;
+  const int i = (int)(item % K.nx2);
+  const int j = (int)(item / K.nx2);
+  const bool interior = i >= 1 && i <= K.nx && j >= 1 && j <= K.ny;
+  double du[NLIVE];
+#pragma unroll
+  for (int k = 0; k < NLIVE; ++k) du[k] = 0.0;
+  if (interior) {
+#pragma unroll
+    for (int n = 0; n < NE; ++n)
+#pragma unroll
+      for (int d = 0; d < NP; ++d)
+        if (live_mode(n, d)) ms[LI(n, d) * CELL_BS + tid] = U[item + K.plane * (d + 10 * n)];
+    // volume term
+#pragma unroll 1
+    for (int a = 0; a < NG; ++a) {
+#pragma unroll 1
+      for (int b = 0; b < NG; ++b) {
+        double v[NE];
+#pragma unroll
+        for (int n = 0; n < NE; ++n) {
+          double acc = 0.0;
+#pragma unroll
+          for (int d = 0; d < NP; ++d)
+            if (live_mode(n, d)) acc = acc + ms[LI(n, d) * CELL_BS + tid] * K.phiG[a][b][d];
+          v[n] = acc;
+        }
+        const double rho = v[0];
+        const double u = v[1] / rho, vv = v[2] / rho, w = v[3] / rho;
+        const double E = v[4], B1 = v[5], B2 = v[6], B3 = v[7];
+        const double BB = sq(B1) + sq(B2) + sq(B3);
+        const double p = K.P.gamma1 * (E - 0.5 * rho * (sq(u) + sq(vv) + sq(w)) - 0.5 * BB);
+        const double S = p + 0.5 * BB;
+        const double T = E + S;
+        const double Kc = u * B1 + vv * B2 + w * B3;
+        double Fx[NE], Fy[NE];
+        Fx[0] = v[1];
+        Fx[1] = rho * sq(u) + S - sq(B1);
+        Fx[2] = rho * u * vv - B1 * B2;
+        Fx[3] = rho * u * w - B1 * B3;
+        Fx[4] = T * u - Kc * B1;
+        Fx[5] = 0.0;
+        Fx[6] = u * B2 - vv * B1;
+        Fx[7] = u * B3 - w * B1;
+        Fy[0] = v[2];
+        Fy[1] = rho * u * vv - B1 * B2;
+        Fy[2] = rho * sq(vv) + S - sq(B2);
+        Fy[3] = rho * vv * w - B2 * B3;
+        Fy[4] = T * vv - Kc * B2;
+        Fy[5] = vv * B1 - u * B2;
+        Fy[6] = 0.0;
+        Fy[7] = vv * B3 - w * B2;
+        const double coef = 0.25 * K.w[a] * K.w[b];
+#pragma unroll
+        for (int d = 1; d < NP; ++d)
+#pragma unroll
+          for (int n = 0; n < NE; ++n)
+            if (live_mode(n, d))
+              du[LI(n, d)] = du[LI(n, d)] + coef * (Fx[n] * K.phix[a][b][d] + Fy[n] * K.phiy[a][b][d]);
+      }
+    }
+    // surface terms in the reference order (x faces, then y faces), mass
+    const long long ox = (i - 1) + 1 + (long long)(K.nx + 1) * (j - 1);  // Fxhat(i,j)
+    const long long oy = (i - 1) + (long long)K.nx * j;                  // Fyhat(i,j)
+#pragma unroll
+    for (int n = 0; n < NE; ++n) {
+      double fr[NG], fl[NG], fu[NG], fd[NG];
+#pragma unroll
+      for (int g = 0; g < NG; ++g) {
+        fr[g] = Fxh[(n * NG + g) * K.fxplane + ox];
+        fl[g] = Fxh[(n * NG + g) * K.fxplane + ox - 1];
+        fu[g] = Fyh[(n * NG + g) * K.fyplane + oy];
+        fd[g] = Fyh[(n * NG + g) * K.fyplane + oy - K.nx];
+      }
+#pragma unroll
+      for (int d = 0; d < NP; ++d) {
+        if (!live_mode(n, d)) continue;
+        double acc = du[LI(n, d)];
+#pragma unroll
+        for (int g = 0; g < NG; ++g) acc = acc - K.cxs * K.w[g] * (fr[g] * K.phiGR[g][d] - fl[g] * K.phiGL[g][d]);
+#pragma unroll
+        for (int g = 0; g < NG; ++g) acc = acc - K.cys * K.w[g] * (fu[g] * K.phiGU[g][d] - fd[g] * K.phiGD[g][d]);
+        du[LI(n, d)] = acc / K.mm[d];
+      }
+    }
+  }
+  if (stage == 0) {
+    if (interior) {
+#pragma unroll
+      for (int n = 0; n < NE; ++n)
+#pragma unroll
+        for (int d = 0; d < NP; ++d)
+          if (live_mode(n, d)) duout[item + K.plane * (d + 10 * n)] = du[LI(n, d)];
+    }
+    return;
+  }
+  const double dt = sc->dt;
+#pragma unroll
+  for (int n = 0; n < NE; ++n)
+#pragma unroll
+    for (int d = 0; d < NP; ++d) {
+      if (!live_mode(n, d)) continue;
+      const long long c = item + K.plane * (d + 10 * n);
+      const double dd = du[LI(n, d)];
+      if (stage == 1) {
+        const double u0 = U[c];
+        U0[c] = u0;
+        UI[c] = u0 + dt * dd;
+      } else if (stage == 2) {
+        const double v = UI[c] + dt * dd;
+        UI[c] = (3.0 / 4.0) * U0[c] + (1.0 / 4.0) * v;
+      } else {
+        const double v = UI[c] + dt * dd;
+        UI[c] = (1.0 / 3.0) * U0[c] + (2.0 / 3.0) * v;
+      }
+    }
+}
+
+// --------------------------------------------------- face-B update -------
+// LhEz.f90:71-96 (dEz1 on x faces, dEz2 on y faces) and the face-B stage
+// combine of RK3.f90. stage 0 writes dEz only (gdf_lhez).
+__global__ void __launch_bounds__(128) k_bface(const __grid_constant__ Consts K, const double* __restrict__ EzRL,
+                                               const double* __restrict__ EzUD, const double* __restrict__ EzV,
+                                               double* __restrict__ BX, double* __restrict__ BX0,
+                                               double* __restrict__ BXI, double* __restrict__ BY,
+                                               double* __restrict__ BY0, double* __restrict__ BYI,
+                                               double* __restrict__ dez1, double* __restrict__ dez2,
+                                               const Scal* __restrict__ sc, int stage) {
+  if (sc && !sc->active) return;
+  const long long item = gtid();
+  const long long nbx = K.fxplane;
+  if (item >= nbx + K.fyplane) return;
+  double dez[3];
+  long long o, fp;
+  double *B, *B0, *BI, *dout;
+  if (item < nbx) {
+    const int i = (int)(item % (K.nx + 1));
+    const int j = (int)(item / (K.nx + 1)) + 1;
+    o = item;
+    fp = K.fxplane;
+    const double v1 = EzV[i + (long long)(K.nx + 1) * j];
+    const double v0 = EzV[i + (long long)(K.nx + 1) * (j - 1)];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      double acc = 0.0;
+#pragma unroll
+      for (int g = 0; g < NG; ++g) acc = acc + 0.5 * K.w[g] * EzRL[g * fp + o] * K.EzyG[g][d];
+      dez[d] = (acc - v1 * K.EzU[d] / K.hy + v0 * K.EzD[d] / K.hy) / K.mmE[d];
+    }
+    B = BX; B0 = BX0; BI = BXI; dout = dez1;
+  } else {
+    const long long k = item - nbx;
+    const int i = (int)(k % K.nx) + 1;
+    const int j = (int)(k / K.nx);
+    o = k;
+    fp = K.fyplane;
+    const double v1 = EzV[i + (long long)(K.nx + 1) * j];
+    const double v0 = EzV[(i - 1) + (long long)(K.nx + 1) * j];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      double acc = 0.0;
+#pragma unroll
+      for (int g = 0; g < NG; ++g) acc = acc - 0.5 * K.w[g] * EzUD[g * fp + o] * K.EzxG[g][d];
+      dez[d] = (acc + v1 * K.EzR[d] / K.hx - v0 * K.EzL[d] / K.hx) / K.mmE[d];
+    }
+    B = BY; B0 = BY0; BI = BYI; dout = dez2;
+  }
+  if (stage == 0) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) dout[o + fp * d] = dez[d];
+    return;
+  }
+  const double dt = sc->dt;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const long long c = o + fp * d;
+    if (stage == 1) {
+      const double b = B[c];
+      B0[c] = b;
+      const double bi = b + dt * dez[d];
+      BI[c] = bi;
+      B[c] = bi;
+    } else if (stage == 2) {
+      const double v = BI[c] + dt * dez[d];
+      const double bii = (3.0 / 4.0) * B0[c] + (1.0 / 4.0) * v;
+      BI[c] = bii;
+      B[c] = bii;
+    } else {
+      const double v = BI[c] + dt * dez[d];
+      B[c] = (1.0 / 3.0) * B0[c] + (2.0 / 3.0) * v;
+    }
+  }
+}
+
+// ------------------------------------------------------------ limiter ----
+// TVB_Limiter_P2.f90:16-121 (characteristic TVB, Jacobi over cells), with
+// KXRCF_Detector.f90 as gate, pp_Limiter.f90, and div_free_Balsara.f90:13-79
+// fused, for one interior cell. S is the pre-limit state (ghosts as the
+// reference leaves them), D receives the limited state.
+constexpr int LIM_BS = 64;
+
+__device__ __forceinline__ void matvec8(const double* A, const double* x, double* y) {
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    double acc = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) acc = acc + A[r + 8 * k] * x[k];
+    y[r] = acc;
+  }
+}
+
+__device__ __forceinline__ void trace8(const Consts& K, const double* __restrict__ S, long long c,
+                                       const double* phi, double* out) {
+#pragma unroll
+  for (int n = 0; n < NE; ++n) {
+    double a = 0.0;
+#pragma unroll
+    for (int d = 0; d < NP; ++d)
+      if (live_mode(n, d)) a = a + S[c + K.plane * (d + 10 * n)] * phi[d];
+    out[n] = a;
+  }
+}
+
+// KXRCF_Detector.f90:187-236 for cell c (interior), given its modes m.
+__device__ bool kxrcf_flag(const Consts& K, const double* __restrict__ S, long long c, const double (*m)[NP],
+                           bool prev) {
+  double I[NE];
+#pragma unroll
+  for (int n = 0; n < NE; ++n) I[n] = 0.0;
+  double Lij = 1e-12;
+  double A[NE], B[NE];
+  const long long pl = K.plane;
+  if (S[c + 1 + pl * 10] < 0) {  // uh(i+1,j,1,2) < 0: right side inflow
+#pragma unroll 1
+    for (int g = 0; g < NG; ++g) {
+      trace8(K, S, c, K.phiGR[g], A);
+      trace8(K, S, c + 1, K.phiGL[g], B);
+#pragma unroll
+      for (int n = 0; n < NE; ++n) I[n] = I[n] + K.hy1 * K.w[g] * (A[n] - B[n]);
+      Lij = Lij + K.hy;
+    }
+  }
+  if (S[c - 1 + pl * 10] > 0) {
+#pragma unroll 1
+    for (int g = 0; g < NG; ++g) {
+      trace8(K, S, c, K.phiGL[g], A);
+      trace8(K, S, c - 1, K.phiGR[g], B);
+#pragma unroll
+      for (int n = 0; n < NE; ++n) I[n] = I[n] + K.hy1 * K.w[g] * (A[n] - B[n]);
+      Lij = Lij + K.hy;
+    }
+  }
+  if (S[c + K.nx2 + pl * 20] < 0) {
+#pragma unroll 1
+    for (int g = 0; g < NG; ++g) {
+      trace8(K, S, c, K.phiGU[g], A);
+      trace8(K, S, c + K.nx2, K.phiGD[g], B);
+#pragma unroll
+      for (int n = 0; n < NE; ++n) I[n] = I[n] + K.hx1 * K.w[g] * (A[n] - B[n]);
+      Lij = Lij + K.hx;
+    }
+  }
+  if (S[c - K.nx2 + pl * 20] > 0) {
+#pragma unroll 1
+    for (int g = 0; g < NG; ++g) {
+      trace8(K, S, c, K.phiGD[g], A);
+      trace8(K, S, c - K.nx2, K.phiGU[g], B);
+#pragma unroll
+      for (int n = 0; n < NE; ++n) I[n] = I[n] + K.hx1 * K.w[g] * (A[n] - B[n]);
+      Lij = Lij + K.hx;
+    }
+  }
+  double uinf[NE];
+#pragma unroll
+  for (int n = 0; n < NE; ++n) uinf[n] = 0.0;
+#pragma unroll 1
+  for (int a = 0; a < NG; ++a)
+#pragma unroll 1
+    for (int b = 0; b < NG; ++b)
+#pragma unroll
+      for (int n = 0; n < NE; ++n) {
+        double v = 0.0;
+#pragma unroll
+        for (int d = 0; d < NP; ++d)
+          if (live_mode(n, d)) v = v + m[n][d] * K.phiG[a][b][d];
+        if (fabs(v) + 1e-12 > uinf[n]) uinf[n] = fabs(v) + 1e-12;
+      }
+  bool flag = prev;
+#pragma unroll
+  for (int n = 0; n < NE; ++n) {
+    const double r = fabs(I[n]) / (K.pow_hxhy * Lij * uinf[n]);
+    if (r >= K.ck) flag = true;
+  }
+  return flag;
+}
+
+// calculate_tq of pp_Limiter.f90:101-126
+__device__ double pp_tq(const Consts& K, const double* ubar, const double* uq) {
+  double ta = 0.0, tb = 1.0;
+  double ut[NE];
+  // bisection on [0,1] to width 1e-14 ends after at most 47 halvings
+#pragma unroll 1
+  for (int it = 0; it < 64 && tb - ta > 1e-14; ++it) {
+    const double tq = 0.5 * (ta + tb);
+#pragma unroll
+    for (int n = 0; n < NE; ++n) ut[n] = tq * uq[n] + (1 - tq) * ubar[n];
+    if (pressure(K.P.gamma, ut) < 1e-12) tb = tq; else ta = tq;
+  }
+  return ta;
+}
+
+// pp_Limiter.f90:10-81 for one cell's modes (in place)
+__device__ void pp_cell(const Consts& K, double (*m)[NP]) {
+  const double epsilon = 1e-13;
+  double eta = 1.0;
+  const double rb = m[0][0];
+#pragma unroll 1
+  for (int a = 0; a < NG; ++a)
+#pragma unroll 1
+    for (int b = 0; b < NG; ++b)
+#pragma unroll
+      for (int s = 0; s < 2; ++s) {
+        double rq = 0.0;
+#pragma unroll
+        for (int d = 0; d < NP; ++d)
+          if (live_mode(0, d)) rq = rq + m[0][d] * K.phiGLL[s][a][b][d];
+        const double eta1 = fabs((rb - epsilon) / (rb - rq));
+        if (eta1 < 1) eta = eta1;
+      }
+  if (eta < 1) {
+    const double f = 0.5 * eta;
+#pragma unroll
+    for (int d = 1; d < NP; ++d) m[0][d] = f * m[0][d];
+  }
+  double ubar[NE];
+#pragma unroll
+  for (int n = 0; n < NE; ++n) ubar[n] = m[n][0];
+  eta = 1.0;
+  double eta1 = 1.0;
+#pragma unroll 1
+  for (int a = 0; a < NG; ++a)
+#pragma unroll 1
+    for (int b = 0; b < NG; ++b)
+#pragma unroll 1
+      for (int s = 0; s < 2; ++s) {
+        double uq[NE];
+#pragma unroll
+        for (int n = 0; n < NE; ++n) {
+          double acc = 0.0;
+#pragma unroll
+          for (int d = 0; d < NP; ++d)
+            if (live_mode(n, d)) acc = acc + m[n][d] * K.phiGLL[s][a][b][d];
+          uq[n] = acc;
+        }
+        const double pq = pressure(K.P.gamma, uq);
+        if (pq < 0) {
+          const double tq = pp_tq(K, ubar, uq);
+          double n1 = 0.0, n2 = 0.0;
+#pragma unroll
+          for (int n = 0; n < NE; ++n) {
+            const double sqv = tq * uq[n] + (1 - tq) * ubar[n];
+            n1 = n1 + sq(sqv - ubar[n]);
+            n2 = n2 + sq(uq[n] - ubar[n]);
+          }
+          eta1 = sqrt(n1) / sqrt(n2);
+        }
+        if (eta1 < eta) eta = eta1;
+      }
+  if (eta < 1) eta = 0.5 * eta;
+#pragma unroll
+  for (int n = 0; n < NE; ++n)
+#pragma unroll
+    for (int d = 1; d < NP; ++d) m[n][d] = eta * m[n][d];
+}
+
+__global__ void __launch_bounds__(LIM_BS) k_limit(const __grid_constant__ Consts K, const double* __restrict__ S,
+                                                  double* __restrict__ D, const double* __restrict__ BX,
+                                                  const double* __restrict__ BY, int32_t* __restrict__ flags,
+                                                  int32_t* __restrict__ trouble, int stage, int divfree,
+                                                  const Scal* __restrict__ gate_sc, Scal* __restrict__ sc) {
+  if (gate_sc && !gate_sc->active) return;
+  const long long item = gtid();
+  if (item >= (long long)K.nx * K.ny) return;
+  const int i = (int)(item % K.nx) + 1;
+  const int j = (int)(item / K.nx) + 1;
+  const long long c = i + (long long)K.nx2 * j;
+  const long long pl = K.plane;
+  double m[NE][NP];
+#pragma unroll
+  for (int n = 0; n < NE; ++n)
+#pragma unroll
+    for (int d = 0; d < NP; ++d) m[n][d] = live_mode(n, d) ? S[c + pl * (d + 10 * n)] : 0.0;
+  int32_t word = 0;
+  bool gate = true;
+  if (K.detector == GDF_DETECT_KXRCF) {
+    const bool prev = K.sticky ? (trouble[item] != 0) : false;
+    gate = kxrcf_flag(K, S, c, m, prev);
+    trouble[item] = gate ? 1 : 0;
+    if (gate) word |= (1 << 24);
+  }
+  if (gate) {
+    const double c23 = 2.0 / 3.0;
+    const double rhoij = m[0][0];
+    const double u1 = m[1][0] / rhoij, u2 = m[2][0] / rhoij, u3 = m[3][0] / rhoij;
+    const double Eij = m[4][0], B1 = m[5][0], B2 = m[6][0], B3 = m[7][0];
+    double R[64], L[64];
+    double DR[NE], DL[NE], Dp[NE], Dm[NE], t1[NE], t2[NE], tu[NE], mod[NE];
+    double Rp[NE], Rm[NE], Up[NE], Um[NE];
+    unsigned change = 0;
+    // x direction
+    eigenmatrix(K.P, 0, rhoij, u1, u2, u3, Eij, B1, B2, B3, R, L);
+#pragma unroll
+    for (int n = 0; n < NE; ++n) {
+      DR[n] = S[c + 1 + pl * (10 * n)] - m[n][0];
+      DL[n] = m[n][0] - S[c - 1 + pl * (10 * n)];
+      Dp[n] = m[n][1] + c23 * m[n][3];
+      Dm[n] = m[n][1] - c23 * m[n][3];
+    }
+    matvec8(L, DR, t1);
+    matvec8(L, DL, t2);
+    matvec8(L, Dp, tu);
+#pragma unroll
+    for (int k = 0; k < NE; ++k) mod[k] = minmod1(tu[k], t1[k], t2[k], K.Mh2x);
+    matvec8(R, mod, Rp);
+#pragma unroll
+    for (int d = 0; d < NE; ++d)
+      if (fabs(Rp[d] - Dp[d]) > 1e-6) change |= 1u << d;
+    matvec8(L, Dm, tu);
+#pragma unroll
+    for (int k = 0; k < NE; ++k) mod[k] = minmod1(tu[k], t1[k], t2[k], K.Mh2x);
+    matvec8(R, mod, Rm);
+#pragma unroll
+    for (int d = 0; d < NE; ++d)
+      if (fabs(Rm[d] - Dm[d]) > 1e-6) change |= 1u << d;
+    // y direction
+    if (K.eig_y_zero_w)
+      eigenmatrix(K.P, 1, rhoij, u1, u2, 0.0, Eij, B1, B2, 0.0, R, L);
+    else
+      eigenmatrix(K.P, 1, rhoij, u1, u2, u3, Eij, B1, B2, B3, R, L);
+#pragma unroll
+    for (int n = 0; n < NE; ++n) {
+      DR[n] = S[c + K.nx2 + pl * (10 * n)] - m[n][0];
+      DL[n] = m[n][0] - S[c - K.nx2 + pl * (10 * n)];
+      Dp[n] = m[n][2] + c23 * m[n][5];
+      Dm[n] = m[n][2] - c23 * m[n][5];
+    }
+    matvec8(L, DR, t1);
+    matvec8(L, DL, t2);
+    matvec8(L, Dp, tu);
+#pragma unroll
+    for (int k = 0; k < NE; ++k) mod[k] = minmod1(tu[k], t1[k], t2[k], K.Mh2y);
+    matvec8(R, mod, Up);
+#pragma unroll
+    for (int d = 0; d < NE; ++d)
+      if (fabs(Up[d] - Dp[d]) > 1e-6) change |= 1u << d;
+    matvec8(L, Dm, tu);
+#pragma unroll
+    for (int k = 0; k < NE; ++k) mod[k] = minmod1(tu[k], t1[k], t2[k], K.Mh2y);
+    matvec8(R, mod, Um);
+#pragma unroll
+    for (int d = 0; d < NE; ++d)
+      if (fabs(Um[d] - Dm[d]) > 1e-6) change |= 1u << d;
+#pragma unroll
+    for (int n = 0; n < NE; ++n) {
+      if (change & (1u << n)) {
+#pragma unroll
+        for (int d = 6; d < NP; ++d) m[n][d] = 0.0;
+        m[n][4] = 0.0;
+        m[n][1] = 0.5 * (Rp[n] + Rm[n]);
+        m[n][2] = 0.5 * (Up[n] + Um[n]);
+        m[n][3] = K.tvb_slope * (Rp[n] - Rm[n]);
+        m[n][5] = K.tvb_slope * (Up[n] - Um[n]);
+      }
+    }
+    word |= (int32_t)change;
+  }
+  if (K.pp) pp_cell(K, m);
+  if (divfree) {
+    // div_free_Balsara.f90:30-75 from the four face polynomials
+    const long long fxp = K.fxplane, fyp = K.fyplane;
+    const long long ox = i + (long long)(K.nx + 1) * (j - 1);
+    const long long oy = (i - 1) + (long long)K.nx * j;
+    const double a0R = BX[ox], a1R = BX[ox + fxp], a2R = BX[ox + 2 * fxp];
+    const double a0L = BX[ox - 1], a1L = BX[ox - 1 + fxp], a2L = BX[ox - 1 + 2 * fxp];
+    const double b0U = BY[oy], b1U = BY[oy + fyp], b2U = BY[oy + 2 * fyp];
+    const double b0D = BY[oy - K.nx], b1D = BY[oy - K.nx + fyp], b2D = BY[oy - K.nx + 2 * fyp];
+    const double rxy = K.rxy, ryx = K.ryx;
+    const double c16 = 1.0 / 6.0, c115 = 1.0 / 15.0, c14 = 1.0 / 4.0, c12 = 1.0 / 2.0;
+#pragma unroll
+    for (int d = 0; d < NP; ++d) { m[5][d] = 0.0; m[6][d] = 0.0; }
+    m[5][0] = c12 * (a0R + a0L) + c16 * rxy * (b1U - b1D);
+    m[5][1] = c12 * (a0R - a0L) + c115 * rxy * (b2U - b2D);
+    m[5][2] = c12 * (a1R + a1L);
+    m[5][3] = -c14 * rxy * (b1U - b1D);
+    m[5][4] = c12 * (a1R - a1L);
+    m[5][5] = c12 * (a2R + a2L);
+    m[5][6] = -c16 * rxy * (b2U - b2D);
+    m[5][8] = c12 * (a2R - a2L);
+    m[6][0] = c12 * (b0U + b0D) + c16 * ryx * (a1R - a1L);
+    m[6][2] = c12 * (b0U - b0D) + c115 * ryx * (a2R - a2L);
+    m[6][1] = c12 * (b1U + b1D);
+    m[6][5] = -c14 * ryx * (a1R - a1L);
+    m[6][4] = c12 * (b1U - b1D);
+    m[6][3] = c12 * (b2U + b2D);
+    m[6][9] = -c16 * ryx * (a2R - a2L);
+    m[6][7] = c12 * (b2U - b2D);
+  }
+#pragma unroll
+  for (int n = 0; n < NE; ++n)
+#pragma unroll
+    for (int d = 0; d < NP; ++d)
+      if (live_mode(n, d)) D[c + pl * (d + 10 * n)] = m[n][d];
+  if (flags) {
+    int32_t w = (word & 0xff) << (8 * (stage - 1));
+    if (word & (1 << 24)) w |= (1 << (23 + stage));
+    if (stage <= 1) flags[item] = w; else flags[item] |= w;
+  }
+  if (!(m[0][0] > 0.0) || !isfinite(m[4][0])) atomicOr(&sc->status, 1);
+}
+
+// Face-B TVB limiter of TVB_Limiter_P2.f90:128-187 (applied when enabled):
+// S holds the limited cell state with ghosts set, pre div-free.
+__device__ __forceinline__ double minmodB(double a, double b, double c, double Mh2) {
+  if (fabs(a) <= Mh2) return a;
+  const double s = (sgn1(a) + sgn1(b) + sgn1(c)) / 3.0;
+  if (fabs(s) == 1) return s * fmin2(fmin2(fabs(a), fabs(b)), fabs(c));
+  return 0.0;
+}
+
+__global__ void k_faceb_limit(const __grid_constant__ Consts K, const double* __restrict__ S,
+                              double* __restrict__ BX, double* __restrict__ BY, const Scal* __restrict__ sc) {
+  if (sc && !sc->active) return;
+  const long long item = gtid();
+  const long long pl = K.plane;
+  const double c23 = 2.0 / 3.0, c25 = 2.0 / 5.0;
+  (void)c25;
+  if (item < K.fxplane) {
+    const int i = (int)(item % (K.nx + 1));
+    const int j = (int)(item / (K.nx + 1)) + 1;
+    const long long cL = i + (long long)K.nx2 * j, cR = cL + 1;
+    const long long s6 = pl * 50;  // Bx slots start at d + 10*5
+    // aRM(i,j,d) (d = 2,3) of cell i and aLM(i+1,j,d) of cell i+1
+    const double aRM2 = S[cL + s6 + pl * 2] + S[cL + s6 + pl * 4];
+    const double aRM3 = S[cL + s6 + pl * 5] + S[cL + s6 + pl * 8];
+    const double aLM2 = S[cR + s6 + pl * 2] - S[cR + s6 + pl * 4];
+    const double aLM3 = S[cR + s6 + pl * 5] - S[cR + s6 + pl * 8];
+    BX[item + K.fxplane] = minmodB(BX[item + K.fxplane], aRM2, aLM2, K.Mh2x_b);
+    BX[item + 2 * K.fxplane] = minmodB(BX[item + 2 * K.fxplane], aRM3, aLM3, K.Mh2x_b);
+    (void)c23;
+  } else if (item < K.fxplane + K.fyplane) {
+    const long long k = item - K.fxplane;
+    const int i = (int)(k % K.nx) + 1;
+    const int j = (int)(k / K.nx);
+    const long long cD = i + (long long)K.nx2 * j, cU = cD + K.nx2;
+    const long long s7 = pl * 60;
+    const double bUM2 = S[cD + s7 + pl * 1] + S[cD + s7 + pl * 4];
+    const double bUM3 = S[cD + s7 + pl * 3] + S[cD + s7 + pl * 7];
+    const double bDM2 = S[cU + s7 + pl * 1] - S[cU + s7 + pl * 4];
+    const double bDM3 = S[cU + s7 + pl * 3] - S[cU + s7 + pl * 7];
+    BY[k + K.fyplane] = minmodB(BY[k + K.fyplane], bUM2, bDM2, K.Mh2y_b);
+    BY[k + 2 * K.fyplane] = minmodB(BY[k + 2 * K.fyplane], bUM3, bDM3, K.Mh2y_b);
+  }
+}
+
+// div_free_Balsara.f90:13-79 on its own (used after the face-B limiter)
+__global__ void k_divfree(const __grid_constant__ Consts K, double* __restrict__ D, const double* __restrict__ BX,
+                          const double* __restrict__ BY, const Scal* __restrict__ sc) {
+  if (sc && !sc->active) return;
+  const long long item = gtid();
+  if (item >= (long long)K.nx * K.ny) return;
+  const int i = (int)(item % K.nx) + 1;
+  const int j = (int)(item / K.nx) + 1;
+  const long long c = i + (long long)K.nx2 * j;
+  const long long pl = K.plane, fxp = K.fxplane, fyp = K.fyplane;
+  const long long ox = i + (long long)(K.nx + 1) * (j - 1);
+  const long long oy = (i - 1) + (long long)K.nx * j;
+  const double a0R = BX[ox], a1R = BX[ox + fxp], a2R = BX[ox + 2 * fxp];
+  const double a0L = BX[ox - 1], a1L = BX[ox - 1 + fxp], a2L = BX[ox - 1 + 2 * fxp];
+  const double b0U = BY[oy], b1U = BY[oy + fyp], b2U = BY[oy + 2 * fyp];
+  const double b0D = BY[oy - K.nx], b1D = BY[oy - K.nx + fyp], b2D = BY[oy - K.nx + 2 * fyp];
+  const double rxy = K.rxy, ryx = K.ryx;
+  const double c16 = 1.0 / 6.0, c115 = 1.0 / 15.0, c14 = 1.0 / 4.0, c12 = 1.0 / 2.0;
+  double* X = D + c + pl * 50;
+  double* Y = D + c + pl * 60;
+  X[0] = c12 * (a0R + a0L) + c16 * rxy * (b1U - b1D);
+  X[pl * 1] = c12 * (a0R - a0L) + c115 * rxy * (b2U - b2D);
+  X[pl * 2] = c12 * (a1R + a1L);
+  X[pl * 3] = -c14 * rxy * (b1U - b1D);
+  X[pl * 4] = c12 * (a1R - a1L);
+  X[pl * 5] = c12 * (a2R + a2L);
+  X[pl * 6] = -c16 * rxy * (b2U - b2D);
+  X[pl * 8] = c12 * (a2R - a2L);
+  Y[0] = c12 * (b0U + b0D) + c16 * ryx * (a1R - a1L);
+  Y[pl * 2] = c12 * (b0U - b0D) + c115 * ryx * (a2R - a2L);
+  Y[pl * 1] = c12 * (b1U + b1D);
+  Y[pl * 5] = -c14 * ryx * (a1R - a1L);
+  Y[pl * 4] = c12 * (b1U - b1D);
+  Y[pl * 3] = c12 * (b2U + b2D);
+  Y[pl * 9] = -c16 * ryx * (a2R - a2L);
+  Y[pl * 7] = c12 * (b2U - b2D);
+}
+
+// --------------------------------------------------------- dt -----------
+// calculate_dt.f90:11-25: per-block maxima of |u_n +- c_f| over the cell
+// averages, then one block folds them and advances t (RK3.f90:60-71).
+constexpr int DT_BS = 256;
+
+__device__ __forceinline__ double max_ign_nan(double a, double b) {
+  if (b != b) return a;
+  if (a != a) return b;
+  return b > a ? b : a;
+}
+
+__global__ void __launch_bounds__(DT_BS) k_dt_partial(const __grid_constant__ Consts K, const double* __restrict__ U,
+                                                      double* __restrict__ part, Scal* __restrict__ sc) {
+  __shared__ double sx[DT_BS], sy[DT_BS];
+  const long long item = gtid();
+  double ax = 0.0, ay = 0.0;
+  if (item < (long long)K.nx * K.ny) {
+    const int i = (int)(item % K.nx) + 1;
+    const int j = (int)(item / K.nx) + 1;
+    const long long c = i + (long long)K.nx2 * j;
+    double Uv[NE];
+#pragma unroll
+    for (int n = 0; n < NE; ++n) Uv[n] = U[c + K.plane * (10 * n)];
+    double a1, a2;
+    fast_speeds(K.P, Uv, 0, a1, a2);
+    if (fabs(a1) > ax || fabs(a2) > ax) ax = fmax2(fabs(a1), fabs(a2));
+    fast_speeds(K.P, Uv, 1, a1, a2);
+    if (fabs(a1) > ay || fabs(a2) > ay) ay = fmax2(fabs(a1), fabs(a2));
+    if (!(Uv[0] > 0.0) || !isfinite(Uv[4])) atomicOr(&sc->status, 1);
+  }
+  sx[threadIdx.x] = ax;
+  sy[threadIdx.x] = ay;
+  __syncthreads();
+  for (int s = DT_BS / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      sx[threadIdx.x] = max_ign_nan(sx[threadIdx.x], sx[threadIdx.x + s]);
+      sy[threadIdx.x] = max_ign_nan(sy[threadIdx.x], sy[threadIdx.x + s]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = sx[0];
+    part[2 * blockIdx.x + 1] = sy[0];
+  }
+}
+
+// mode 0: gdf_dt (dt only); mode 1: a time step (t update, active flag)
+__global__ void __launch_bounds__(DT_BS) k_dt_final(const __grid_constant__ Consts K, const double* __restrict__ part,
+                                                    int nblocks, Scal* __restrict__ sc, int mode) {
+  __shared__ double sx[DT_BS], sy[DT_BS];
+  double ax = 0.0, ay = 0.0;
+  for (int b = threadIdx.x; b < nblocks; b += DT_BS) {
+    ax = max_ign_nan(ax, part[2 * b]);
+    ay = max_ign_nan(ay, part[2 * b + 1]);
+  }
+  sx[threadIdx.x] = ax;
+  sy[threadIdx.x] = ay;
+  __syncthreads();
+  for (int s = DT_BS / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      sx[threadIdx.x] = max_ign_nan(sx[threadIdx.x], sx[threadIdx.x + s]);
+      sy[threadIdx.x] = max_ign_nan(sy[threadIdx.x], sy[threadIdx.x + s]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  double dt = K.cfl / (sx[0] / K.hx + sy[0] / K.hy);
+  if (mode == 0) {
+    sc->dt = dt;
+    return;
+  }
+  double t = sc->t;
+  if (!(t < sc->tend)) {
+    sc->active = 0;
+    return;
+  }
+  if (t + dt >= sc->tend) {
+    dt = sc->tend - t;
+    t = sc->tend;
+  } else {
+    t = t + dt;
+  }
+  if (K.dt_floor_stop && dt < 1e-7) t = sc->tend;
+  if (!(dt > 0.0) || !isfinite(dt)) sc->status |= 1;
+  sc->dt = dt;
+  sc->t = t;
+  sc->active = 1;
+  sc->steps += 1;
+}
+
+// ------------------------------------------------------ diagnostics -------
+// calculate_umax.f90, calculate_totaldiv.f90, calculate_pmin.f90, and the
+// number of flagged cells. Per-block partials, folded by k_diag_final.
+__global__ void __launch_bounds__(DT_BS) k_diag_partial(const __grid_constant__ Consts K, const double* __restrict__ U,
+                                                        const int32_t* __restrict__ flags, double* __restrict__ part) {
+  __shared__ double s_um[DT_BS], s_td[DT_BS], s_pm[DT_BS], s_nt[DT_BS];
+  const long long item = gtid();
+  double um = 0.0, td = 0.0, pm = 1000000.0, nt = 0.0;
+  if (item < (long long)K.nx * K.ny) {
+    const int i = (int)(item % K.nx) + 1;
+    const int j = (int)(item / K.nx) + 1;
+    const long long c = i + (long long)K.nx2 * j;
+    double m[NE][NP];
+#pragma unroll
+    for (int n = 0; n < NE; ++n)
+#pragma unroll
+      for (int d = 0; d < NP; ++d) m[n][d] = live_mode(n, d) ? U[c + K.plane * (d + 10 * n)] : 0.0;
+    if (K.umax_all) {
+#pragma unroll
+      for (int n = 0; n < NE; ++n)
+        if (fabs(m[n][0]) > um) um = fabs(m[n][0]);
+    } else {
+      um = fabs(m[0][0]);
+    }
+#pragma unroll 1
+    for (int a = 0; a < NG; ++a)
+#pragma unroll 1
+      for (int b = 0; b < NG; ++b) {
+        double gd = 0.0;
+#pragma unroll
+        for (int d = 0; d < NP; ++d) gd = gd + m[5][d] * K.phix[a][b][d] + m[6][d] * K.phiy[a][b][d];
+        td = td + K.w[a] * K.w[b] * sq(gd);
+        double q[NE];
+#pragma unroll
+        for (int n = 0; n < NE; ++n) {
+          double acc = 0.0;
+#pragma unroll
+          for (int d = 0; d < NP; ++d)
+            if (live_mode(n, d)) acc = acc + m[n][d] * K.phiG[a][b][d];
+          q[n] = acc;
+        }
+        const double p1 = pressure(K.P.gamma, q);
+        if (p1 < pm) pm = p1;
+      }
+    if (flags && flags[item] != 0) nt = 1.0;
+  }
+  s_um[threadIdx.x] = um; s_td[threadIdx.x] = td; s_pm[threadIdx.x] = pm; s_nt[threadIdx.x] = nt;
+  __syncthreads();
+  for (int s = DT_BS / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      s_um[threadIdx.x] = fmax(s_um[threadIdx.x], s_um[threadIdx.x + s]);
+      s_td[threadIdx.x] = s_td[threadIdx.x] + s_td[threadIdx.x + s];
+      s_pm[threadIdx.x] = fmin(s_pm[threadIdx.x], s_pm[threadIdx.x + s]);
+      s_nt[threadIdx.x] = s_nt[threadIdx.x] + s_nt[threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[4 * blockIdx.x] = s_um[0];
+    part[4 * blockIdx.x + 1] = s_td[0];
+    part[4 * blockIdx.x + 2] = s_pm[0];
+    part[4 * blockIdx.x + 3] = s_nt[0];
+  }
+}
+
+__global__ void k_diag_final(const __grid_constant__ Consts K, const double* __restrict__ part, int nblocks,
+                             Scal* __restrict__ sc) {
+  if (threadIdx.x != 0) return;
+  double um = 0.0, td = 0.0, pm = 1000000.0, nt = 0.0;
+  for (int b = 0; b < nblocks; ++b) {
+    um = fmax(um, part[4 * b]);
+    td = td + part[4 * b + 1];
+    pm = fmin(pm, part[4 * b + 2]);
+    nt = nt + part[4 * b + 3];
+  }
+  sc->umax = um;
+  sc->totaldiv = sqrt(td * K.hx1 * K.hy1);
+  sc->pmin = pm;
+  sc->troubled = (long long)nt;
+}
+
+}  // namespace gdf
+
+// =====================================================================
+// Host side: handle, constants, C ABI.
+// =====================================================================
+using namespace gdf;
+
+static thread_local std::string g_err;
+
+static int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CK(call)                                                                       \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess) return fail(GDF_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
+  } while (0)
+
+struct GdfHandle {
+  GdfConfig cfg{};
+  Consts K{};
+  cudaStream_t st = nullptr;
+  double *U = nullptr, *U0 = nullptr, *UI = nullptr, *UT = nullptr;
+  double *BX = nullptr, *BX0 = nullptr, *BXI = nullptr, *BY = nullptr, *BY0 = nullptr, *BYI = nullptr;
+  double *Fxh = nullptr, *Fyh = nullptr, *EzRL = nullptr, *EzUD = nullptr, *EzV = nullptr;
+  double *part = nullptr;
+  int32_t *flags = nullptr, *trouble = nullptr;
+  Scal* sc = nullptr;
+  Scal* sc_host = nullptr;  // pinned mirror
+  int uploaded = 0;
+  int64_t launches = 0;
+  int64_t step_launches = 0;
+  int dt_blocks = 0;
+  cudaGraphExec_t graph = nullptr;
+  // per-kernel timing (gdf_profile): events around every launch when set
+  int prof = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double prof_ms[GDF_KERNEL_KINDS] = {0};
+  int64_t prof_n[GDF_KERNEL_KINDS] = {0};
+};
+
+// Record a launch: when profiling, bracket it with events on the handle's
+// stream and accumulate its device time under its kind.
+template <class F>
+static int run_kernel(GdfHandle* h, int kind, F&& launch) {
+  if (h->prof) cudaEventRecord(h->ev0, h->st);
+  launch();
+  h->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(GDF_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+  if (h->prof) {
+    cudaEventRecord(h->ev1, h->st);
+    cudaEventSynchronize(h->ev1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    h->prof_ms[kind] += ms;
+    h->prof_n[kind] += 1;
+  }
+  return GDF_OK;
+}
+
+static void build_consts(const GdfConfig& c, Consts& K) {
+  std::memset(&K, 0, sizeof(K));
+  K.nx = c.nx; K.ny = c.ny; K.nx2 = c.nx + 2; K.ny2 = c.ny + 2;
+  K.plane = (long long)K.nx2 * K.ny2;
+  K.fxplane = (long long)(c.nx + 1) * c.ny;
+  K.fyplane = (long long)c.nx * (c.ny + 1);
+  K.vplane = (long long)(c.nx + 1) * (c.ny + 1);
+  // init_data.f90:21-24
+  K.hx = (c.xb - c.xa) / c.nx;
+  K.hy = (c.yb - c.ya) / c.ny;
+  K.hx1 = 0.5 * K.hx;
+  K.hy1 = 0.5 * K.hy;
+  K.cxs = 0.5 / K.hx;
+  K.cys = 0.5 / K.hy;
+  K.Mh2x = c.tvb_m * (K.hx * K.hx);
+  K.Mh2y = c.tvb_m * (K.hy * K.hy);
+  K.Mh2x_b = c.tvb_m * (K.hy * K.hy);
+  K.Mh2y_b = c.tvb_m * (K.hx * K.hx);
+  K.rxy = K.hx / K.hy;
+  K.ryx = K.hy / K.hx;
+  K.tvb_slope = c.tvb_slope;
+  K.cfl = c.cfl;
+  K.ck = c.kxrcf_ck;
+  K.pow_hxhy = std::pow(K.hx * K.hy, 0.25 * (2 + 1));  // KXRCF_Detector.f90:98
+  K.bc_r = c.bc_r; K.bc_l = c.bc_l; K.bc_u = c.bc_u; K.bc_d = c.bc_d;
+  K.pp = c.pp_limiter; K.faceb = c.faceb_limiter; K.ez_fhat = c.ez_face_fhat;
+  K.eig_y_zero_w = c.eig_y_zero_w; K.detector = c.detector; K.sticky = c.kxrcf_sticky;
+  K.dt_floor_stop = c.dt_floor_stop; K.umax_all = c.umax_all_vars;
+  K.P.gamma = c.gamma;
+  K.P.gamma1 = c.gamma - 1;
+  K.P.gflux = c.gamma_flux;
+  K.P.hlld_eps = c.hlld_eps;
+  K.P.flux = c.flux_type;
+  K.P.kml_w = c.kml_w_term;
+  K.P.eig_p_typo = c.eig_p_typo;
+  K.P.eig_identity = c.eig_identity;
+  // get_GLP.f90:38-56 (5-point branch)
+  const double lam[NG] = {-0.9061798459386639927976269, -0.5384693101056830910363144, 0,
+                          0.5384693101056830910363144, 0.9061798459386639927976269};
+  const double wt[NG] = {0.2369268850561890875142640, 0.4786286704993664680412915, 0.5688888888888888888888889,
+                         0.4786286704993664680412915, 0.2369268850561890875142640};
+  const double lamL[NG] = {-1, -0.6546536707079771437983, 0, 0.654653670707977143798, 1};
+  const double hx1 = K.hx1, hy1 = K.hy1;
+  const double c13 = 1.0 / 3.0, c23 = 2.0 / 3.0, c25 = 2.0 / 5.0, c35 = 3.0 / 5.0;
+  for (int a = 0; a < NG; ++a) { K.w[a] = wt[a]; K.lam[a] = lam[a]; }
+  // get_basis.f90: Legendre tensor basis values and derivatives
+  auto P2 = [&](double x) { return x * x - c13; };
+  auto P3 = [&](double x) { return x * x * x - 3.0 * x / 5.0; };
+  for (int a = 0; a < NG; ++a)
+    for (int b = 0; b < NG; ++b) {
+      const double li = lam[a], lj = lam[b], Li = lamL[a], Lj = lamL[b];
+      double* G = K.phiG[a][b];
+      double* X = K.phix[a][b];
+      double* Y = K.phiy[a][b];
+      double* G1 = K.phiGLL[0][a][b];
+      double* G2 = K.phiGLL[1][a][b];
+      G[0] = 1; G1[0] = 1; G2[0] = 1; X[0] = 0; Y[0] = 0;
+      G[1] = li; G1[1] = Li; G2[1] = li; X[1] = 1.0 / hx1; Y[1] = 0;
+      G[2] = lj; G1[2] = lj; G2[2] = Lj; X[2] = 0; Y[2] = 1.0 / hy1;
+      G[3] = P2(li); G1[3] = P2(Li); G2[3] = P2(li); X[3] = 2.0 * li / hx1; Y[3] = 0;
+      G[4] = li * lj; G1[4] = Li * lj; G2[4] = li * Lj; X[4] = lj / hx1; Y[4] = li / hy1;
+      G[5] = P2(lj); G1[5] = P2(lj); G2[5] = P2(Lj); X[5] = 0; Y[5] = 2.0 * lj / hy1;
+      G[6] = P3(li); G1[6] = P3(Li); G2[6] = P3(li); X[6] = (3 * (li * li) - c35) / hx1; Y[6] = 0;
+      G[7] = P2(li) * lj; G1[7] = P2(Li) * lj; G2[7] = P2(li) * Lj;
+      X[7] = 2.0 * li * lj / hx1; Y[7] = P2(li) / hy1;
+      G[8] = li * P2(lj); G1[8] = Li * P2(lj); G2[8] = li * P2(Lj);
+      X[8] = P2(lj) / hx1; Y[8] = 2.0 * li * lj / hy1;
+      G[9] = P3(lj); G1[9] = P3(lj); G2[9] = P3(Lj); X[9] = 0; Y[9] = (3 * (lj * lj) - c35) / hy1;
+    }
+  for (int g = 0; g < NG; ++g) {
+    const double l = lam[g];
+    const double R[NP] = {1, 1, l, c23, l, P2(l), c25, c23 * l, P2(l), P3(l)};
+    const double Lf[NP] = {1, -1, l, c23, -l, P2(l), -c25, c23 * l, -P2(l), P3(l)};
+    const double Uf[NP] = {1, l, 1, P2(l), l, c23, P3(l), P2(l), l * c23, c25};
+    const double Df[NP] = {1, l, -1, P2(l), -l, c23, P3(l), -P2(l), l * c23, -c25};
+    for (int d = 0; d < NP; ++d) {
+      K.phiGR[g][d] = R[d]; K.phiGL[g][d] = Lf[d]; K.phiGU[g][d] = Uf[d]; K.phiGD[g][d] = Df[d];
+    }
+    K.EzxG[g][0] = 0; K.EzxG[g][1] = 1 / hx1; K.EzxG[g][2] = 2 * l / hx1;
+    K.EzyG[g][0] = 0; K.EzyG[g][1] = 1 / hy1; K.EzyG[g][2] = 2 * l / hy1;
+  }
+  const double ru[NP] = {1, 1, 1, c23, 1, c23, c25, c23, c23, c25};
+  const double lu[NP] = {1, -1, 1, c23, -1, c23, -c25, c23, -c23, c25};
+  const double rd[NP] = {1, 1, -1, c23, -1, c23, c25, -c23, c23, -c25};
+  const double ld[NP] = {1, -1, -1, c23, 1, c23, -c25, -c23, -c23, -c25};
+  const double mm[NP] = {1, 1.0 / 3.0, 1.0 / 3.0, 4.0 / 45.0, 1.0 / 9.0, 4.0 / 45.0,
+                         4.0 / 175.0, 4.0 / 135.0, 4.0 / 135.0, 4.0 / 175.0};
+  for (int d = 0; d < NP; ++d) {
+    K.phiRU[d] = ru[d]; K.phiLU[d] = lu[d]; K.phiRD[d] = rd[d]; K.phiLD[d] = ld[d]; K.mm[d] = mm[d];
+  }
+  K.mmE[0] = 1; K.mmE[1] = 1.0 / 3.0; K.mmE[2] = 4.0 / 45.0;
+  K.EzR[0] = 1; K.EzR[1] = 1; K.EzR[2] = c23;
+  K.EzL[0] = 1; K.EzL[1] = -1; K.EzL[2] = c23;
+  for (int d = 0; d < 3; ++d) { K.EzU[d] = K.EzR[d]; K.EzD[d] = K.EzL[d]; }
+}
+
+static int check_config(const GdfConfig* c) {
+  if (!c) return fail(GDF_ERR_ARG, "null config");
+  if (c->nx < 2 || c->ny < 2) return fail(GDF_ERR_ARG, "nx and ny must be >= 2");
+  if ((long long)c->nx * c->ny > (1LL << 31)) return fail(GDF_ERR_ARG, "grid too large");
+  if (!(c->xb > c->xa) || !(c->yb > c->ya)) return fail(GDF_ERR_ARG, "empty domain");
+  const int bcs[4] = {c->bc_r, c->bc_l, c->bc_u, c->bc_d};
+  for (int b : bcs)
+    if (b != GDF_BC_PERIODIC && b != GDF_BC_OUTFLOW) return fail(GDF_ERR_ARG, "boundary must be 1 or 2");
+  if (c->flux_type < 1 || c->flux_type > 4) return fail(GDF_ERR_ARG, "flux_type must be 1..4");
+  if (!(c->gamma > 1.0) || !(c->gamma_flux > 1.0)) return fail(GDF_ERR_ARG, "gamma must be > 1");
+  if (!(c->cfl > 0.0)) return fail(GDF_ERR_ARG, "cfl must be > 0");
+  if (c->detector != GDF_DETECT_ALL && c->detector != GDF_DETECT_KXRCF) return fail(GDF_ERR_ARG, "unknown detector");
+  return GDF_OK;
+}
+
+static inline unsigned nblk(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+#define LAUNCH_CHECK(h)                                                                   \
+  do {                                                                                    \
+    cudaError_t e_ = cudaGetLastError();                                                  \
+    if (e_ != cudaSuccess) return fail(GDF_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e_)); \
+  } while (0)
+
+static int launch_set_bc(GdfHandle* h, double* U, int zeroB, const Scal* sc) {
+  const long long n = (2LL * (h->K.nx + 2) + 2LL * h->K.ny) * NLIVE;
+  return run_kernel(h, GDF_K_SET_BC, [&] { k_set_bc<<<nblk(n, 256), 256, 0, h->st>>>(h->K, U, zeroB, sc); });
+}
+
+// Lh traces/Riemann (Fxhat, Fyhat, EzRL, EzUD) and LhEz vertex Ez on U
+static int launch_faces(GdfHandle* h, const double* U, const Scal* sc) {
+  const Consts& K = h->K;
+  const long long nfx = (long long)(K.nx + 1) * NG * K.ny;
+  const long long nfy = (long long)K.nx * NG * (K.ny + 1);
+  int rc = run_kernel(h, GDF_K_FACE_X, [&] { k_face<0><<<nblk(nfx, 128), 128, 0, h->st>>>(K, U, h->Fxh, h->EzRL, sc); });
+  if (!rc) rc = run_kernel(h, GDF_K_FACE_Y, [&] { k_face<1><<<nblk(nfy, 128), 128, 0, h->st>>>(K, U, h->Fyh, h->EzUD, sc); });
+  if (!rc) rc = run_kernel(h, GDF_K_VERTEX, [&] { k_vertex<<<nblk(K.vplane, 128), 128, 0, h->st>>>(K, U, h->EzV, sc); });
+  return rc;
+}
+
+static int launch_dt(GdfHandle* h, const double* U, int mode) {
+  int rc = run_kernel(h, GDF_K_DT, [&] { k_dt_partial<<<h->dt_blocks, DT_BS, 0, h->st>>>(h->K, U, h->part, h->sc); });
+  if (!rc) rc = run_kernel(h, GDF_K_DT, [&] { k_dt_final<<<1, DT_BS, 0, h->st>>>(h->K, h->part, h->dt_blocks, h->sc, mode); });
+  return rc;
+}
+
+static int launch_limit(GdfHandle* h, const double* S, double* D, int stage, const Scal* sc_gate) {
+  const Consts& K = h->K;
+  const long long ncell = (long long)K.nx * K.ny;
+  const int fused_divfree = K.faceb ? 0 : 1;
+  int rc0 = run_kernel(h, GDF_K_LIMIT, [&] {
+    k_limit<<<nblk(ncell, LIM_BS), LIM_BS, 0, h->st>>>(K, S, D, h->BX, h->BY, h->flags, h->trouble, stage,
+                                                       fused_divfree, sc_gate, h->sc);
+  });
+  if (rc0) return rc0;
+  if (K.faceb) {
+    // TVB_Limiter_P2.f90:126-187 then div_free: set_bc on the limited state,
+    // face-B minmod, div-free reconstruction
+    int rc = launch_set_bc(h, D, 0, sc_gate);
+    if (rc) return rc;
+    rc = run_kernel(h, GDF_K_LIMIT, [&] {
+      k_faceb_limit<<<nblk(K.fxplane + K.fyplane, 128), 128, 0, h->st>>>(K, D, h->BX, h->BY, sc_gate);
+    });
+    if (!rc) rc = run_kernel(h, GDF_K_LIMIT, [&] { k_divfree<<<nblk(ncell, 128), 128, 0, h->st>>>(K, D, h->BX, h->BY, sc_gate); });
+    if (rc) return rc;
+  }
+  return GDF_OK;
+}
+
+// One RK3 stage on the resident state (stage = 1, 2, 3).
+static int launch_stage(GdfHandle* h, int stage) {
+  const Consts& K = h->K;
+  int rc;
+  if (stage == 1) {
+    if ((rc = launch_set_bc(h, h->U, 0, h->sc))) return rc;  // RK3.f90:74
+  }
+  if ((rc = launch_faces(h, h->U, h->sc))) return rc;
+  rc = run_kernel(h, GDF_K_CELL, [&] {
+    k_cell<<<nblk(K.plane, CELL_BS), CELL_BS, 0, h->st>>>(K, h->U, h->U0, h->UI, h->Fxh, h->Fyh, nullptr, h->sc, stage);
+  });
+  if (!rc) rc = run_kernel(h, GDF_K_BFACE, [&] {
+    k_bface<<<nblk(K.fxplane + K.fyplane, 128), 128, 0, h->st>>>(K, h->EzRL, h->EzUD, h->EzV, h->BX, h->BX0, h->BXI,
+                                                                 h->BY, h->BY0, h->BYI, nullptr, nullptr, h->sc, stage);
+  });
+  if (rc) return rc;
+  if ((rc = launch_limit(h, h->UI, h->U, stage, h->sc))) return rc;
+  // RK3.f90:97 / :123 set_bc after stages 1 and 2; after stage 3 the ghosts
+  // are TVB_Limiter_P2's set_bc with div_free's zeroed B modes
+  return launch_set_bc(h, h->U, stage == 3 ? 1 : 0, h->sc);
+}
+
+static int launch_step(GdfHandle* h) {
+  int rc = launch_dt(h, h->U, 1);
+  if (rc) return rc;
+  for (int s = 1; s <= 3; ++s)
+    if ((rc = launch_stage(h, s))) return rc;
+  return GDF_OK;
+}
+
+static int sync_scal(GdfHandle* h) {
+  CK(cudaMemcpyAsync(h->sc_host, h->sc, sizeof(Scal), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return GDF_OK;
+}
+
+static size_t uh_bytes(const GdfConfig& c) { return (size_t)(c.nx + 2) * (c.ny + 2) * NP * NE * sizeof(double); }
+static size_t bx_bytes(const GdfConfig& c) { return (size_t)(c.nx + 1) * c.ny * 3 * sizeof(double); }
+static size_t by_bytes(const GdfConfig& c) { return (size_t)c.nx * (c.ny + 1) * 3 * sizeof(double); }
+
+// dead (mode, variable) slots must be zero in an uploaded state
+static int check_dead_slots(const GdfConfig& c, const double* uh) {
+  const size_t plane = (size_t)(c.nx + 2) * (c.ny + 2);
+  for (int n = 0; n < NE; ++n)
+    for (int d = 0; d < NP; ++d) {
+      if (live_mode(n, d)) continue;
+      const double* p = uh + plane * (d + 10 * n);
+      for (size_t q = 0; q < plane; ++q)
+        if (p[q] != 0.0)
+          return fail(GDF_ERR_ARG, "uh has a nonzero value in mode " + std::to_string(d + 1) + " of variable " +
+                                       std::to_string(n + 1) + ", which the P2 scheme never populates");
+    }
+  return GDF_OK;
+}
+
+// Capture one time step (RK3.f90:60-151) of the resident state as a CUDA
+// graph; replays need no host work between steps.
+static int ensure_graph(GdfHandle* h) {
+  if (h->graph) return GDF_OK;
+  cudaGraph_t g;
+  CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+  const int64_t l0 = h->launches;
+  int rc = launch_step(h);
+  h->step_launches = h->launches - l0;
+  h->launches = l0;
+  cudaError_t e = cudaStreamEndCapture(h->st, &g);
+  if (rc) return rc;
+  if (e != cudaSuccess) return fail(GDF_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&h->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    h->graph = nullptr;
+    return fail(GDF_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  }
+  return GDF_OK;
+}
+
+extern "C" {
+
+const char* gdf_last_error(void) { return g_err.c_str(); }
+
+int gdf_build_exact(void) { return GDF_EXACT; }
+
+int64_t gdf_kernel_launches(GdfHandle* h) { return h ? h->launches : -1; }
+
+int gdf_create(const GdfConfig* cfg, GdfHandle** out) {
+  if (!out) return fail(GDF_ERR_ARG, "null handle pointer");
+  *out = nullptr;
+  int rc = check_config(cfg);
+  if (rc) return rc;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(GDF_ERR_CUDA, "no CUDA device available");
+  }
+  GdfHandle* h = new GdfHandle();
+  h->cfg = *cfg;
+  build_consts(*cfg, h->K);
+  const GdfConfig& c = *cfg;
+  const size_t ub = uh_bytes(c), bxb = bx_bytes(c), byb = by_bytes(c);
+  const size_t fxb = (size_t)h->K.fxplane * NG * NE * sizeof(double);
+  const size_t fyb = (size_t)h->K.fyplane * NG * NE * sizeof(double);
+  const long long ncell = (long long)c.nx * c.ny;
+  h->dt_blocks = (int)nblk(ncell, DT_BS);
+  auto alloc = [&](void** p, size_t bytes) -> bool {
+    if (cudaMalloc(p, bytes) != cudaSuccess) return false;
+    return cudaMemset(*p, 0, bytes) == cudaSuccess;
+  };
+  bool ok = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) == cudaSuccess;
+  ok = ok && alloc((void**)&h->U, ub) && alloc((void**)&h->U0, ub) && alloc((void**)&h->UI, ub) &&
+       alloc((void**)&h->UT, ub);
+  ok = ok && alloc((void**)&h->BX, bxb) && alloc((void**)&h->BX0, bxb) && alloc((void**)&h->BXI, bxb);
+  ok = ok && alloc((void**)&h->BY, byb) && alloc((void**)&h->BY0, byb) && alloc((void**)&h->BYI, byb);
+  ok = ok && alloc((void**)&h->Fxh, fxb) && alloc((void**)&h->Fyh, fyb);
+  ok = ok && alloc((void**)&h->EzRL, (size_t)h->K.fxplane * NG * sizeof(double)) &&
+       alloc((void**)&h->EzUD, (size_t)h->K.fyplane * NG * sizeof(double)) &&
+       alloc((void**)&h->EzV, (size_t)h->K.vplane * sizeof(double));
+  ok = ok && alloc((void**)&h->part, (size_t)(h->dt_blocks + 1) * 4 * sizeof(double));
+  ok = ok && alloc((void**)&h->flags, (size_t)ncell * sizeof(int32_t)) &&
+       alloc((void**)&h->trouble, (size_t)ncell * sizeof(int32_t));
+  ok = ok && alloc((void**)&h->sc, sizeof(Scal));
+  ok = ok && cudaMallocHost((void**)&h->sc_host, sizeof(Scal)) == cudaSuccess;
+  if (!ok) {
+    cudaGetLastError();
+    gdf_destroy(h);
+    return fail(GDF_ERR_NOMEM, "device allocation failed for a " + std::to_string(c.nx) + "x" +
+                                   std::to_string(c.ny) + " grid");
+  }
+  std::memset(h->sc_host, 0, sizeof(Scal));
+  h->sc_host->tend = 1e300;
+  h->sc_host->active = 1;
+  if (cudaMemcpy(h->sc, h->sc_host, sizeof(Scal), cudaMemcpyHostToDevice) != cudaSuccess) {
+    gdf_destroy(h);
+    return fail(GDF_ERR_CUDA, "initialising device scalars failed");
+  }
+  *out = h;
+  return GDF_OK;
+}
+
+int gdf_destroy(GdfHandle* h) {
+  if (!h) return GDF_OK;
+  if (h->graph) cudaGraphExecDestroy(h->graph);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  double* bufs[] = {h->U, h->U0, h->UI, h->UT, h->BX, h->BX0, h->BXI, h->BY, h->BY0, h->BYI,
+                    h->Fxh, h->Fyh, h->EzRL, h->EzUD, h->EzV, h->part};
+  for (double* p : bufs)
+    if (p) cudaFree(p);
+  if (h->flags) cudaFree(h->flags);
+  if (h->trouble) cudaFree(h->trouble);
+  if (h->sc) cudaFree(h->sc);
+  if (h->sc_host) cudaFreeHost(h->sc_host);
+  if (h->st) cudaStreamDestroy(h->st);
+  delete h;
+  return GDF_OK;
+}
+
+int gdf_upload(GdfHandle* h, const double* uh, const double* bx, const double* by) {
+  if (!h || !uh || !bx || !by) return fail(GDF_ERR_ARG, "null argument");
+  int rc = check_dead_slots(h->cfg, uh);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(h->U, uh, uh_bytes(h->cfg), cudaMemcpyHostToDevice, h->st));
+  CK(cudaMemcpyAsync(h->BX, bx, bx_bytes(h->cfg), cudaMemcpyHostToDevice, h->st));
+  CK(cudaMemcpyAsync(h->BY, by, by_bytes(h->cfg), cudaMemcpyHostToDevice, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  h->uploaded = 1;
+  return GDF_OK;
+}
+
+int gdf_download(GdfHandle* h, double* uh, double* bx, double* by) {
+  if (!h) return fail(GDF_ERR_ARG, "null handle");
+  if (!h->uploaded) return fail(GDF_ERR_STATE, "no state uploaded");
+  if (uh) CK(cudaMemcpyAsync(uh, h->U, uh_bytes(h->cfg), cudaMemcpyDeviceToHost, h->st));
+  if (bx) CK(cudaMemcpyAsync(bx, h->BX, bx_bytes(h->cfg), cudaMemcpyDeviceToHost, h->st));
+  if (by) CK(cudaMemcpyAsync(by, h->BY, by_bytes(h->cfg), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return GDF_OK;
+}
+
+int gdf_set_time(GdfHandle* h, double t) {
+  if (!h) return fail(GDF_ERR_ARG, "null handle");
+  int rc = sync_scal(h);
+  if (rc) return rc;
+  h->sc_host->t = t;
+  CK(cudaMemcpyAsync(h->sc, h->sc_host, sizeof(Scal), cudaMemcpyHostToDevice, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return GDF_OK;
+}
+
+int gdf_get_time(GdfHandle* h, double* t, double* dt) {
+  if (!h) return fail(GDF_ERR_ARG, "null handle");
+  int rc = sync_scal(h);
+  if (rc) return rc;
+  if (t) *t = h->sc_host->t;
+  if (dt) *dt = h->sc_host->dt;
+  return GDF_OK;
+}
+
+static int set_scal(GdfHandle* h, double t, double tend, int active) {
+  int rc = sync_scal(h);
+  if (rc) return rc;
+  h->sc_host->t = t;
+  h->sc_host->tend = tend;
+  h->sc_host->active = active;
+  h->sc_host->status = 0;
+  CK(cudaMemcpyAsync(h->sc, h->sc_host, sizeof(Scal), cudaMemcpyHostToDevice, h->st));
+  return GDF_OK;
+}
+
+int gdf_prepare(GdfHandle* h, int32_t* flags) {
+  if (!h) return fail(GDF_ERR_ARG, "null handle");
+  if (!h->uploaded) return fail(GDF_ERR_STATE, "no state uploaded");
+  int rc = set_scal(h, 0.0, h->sc_host->tend, 1);
+  if (rc) return rc;
+  // RK3.f90:8-12: set_bc, TVB_Limiter_P2, div_free_Balsara
+  if ((rc = launch_set_bc(h, h->U, 0, nullptr))) return rc;
+  CK(cudaMemcpyAsync(h->UI, h->U, uh_bytes(h->cfg), cudaMemcpyDeviceToDevice, h->st));
+  if ((rc = launch_limit(h, h->UI, h->U, 1, nullptr))) return rc;
+  if ((rc = launch_set_bc(h, h->U, 1, nullptr))) return rc;
+  if (flags) {
+    CK(cudaMemcpyAsync(flags, h->flags, (size_t)h->cfg.nx * h->cfg.ny * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                       h->st));
+  }
+  rc = sync_scal(h);
+  if (rc) return rc;
+  if (h->sc_host->status) return fail(GDF_ERR_NUMERIC, "non-positive density or non-finite energy after limiting");
+  return GDF_OK;
+}
+
+int gdf_step(GdfHandle* h, double tend, double* t, double* dt_out, int32_t* flags) {
+  if (!h || !t) return fail(GDF_ERR_ARG, "null argument");
+  if (!h->uploaded) return fail(GDF_ERR_STATE, "no state uploaded");
+  int rc = set_scal(h, *t, tend, 1);
+  if (rc) return rc;
+  if ((rc = launch_step(h))) return rc;
+  if (flags) {
+    CK(cudaMemcpyAsync(flags, h->flags, (size_t)h->cfg.nx * h->cfg.ny * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                       h->st));
+  }
+  if ((rc = sync_scal(h))) return rc;
+  *t = h->sc_host->t;
+  if (dt_out) *dt_out = h->sc_host->dt;
+  if (h->sc_host->status) return fail(GDF_ERR_NUMERIC, "non-finite or non-positive state or dt in this step");
+  return GDF_OK;
+}
+
+int gdf_advance(GdfHandle* h, double tend, int32_t max_steps, double* t, int32_t* steps) {
+  if (!h || !t) return fail(GDF_ERR_ARG, "null argument");
+  if (!h->uploaded) return fail(GDF_ERR_STATE, "no state uploaded");
+  if (max_steps < 0) return fail(GDF_ERR_ARG, "max_steps < 0");
+  int rc = set_scal(h, *t, tend, 1);
+  if (rc) return rc;
+  const long long s0 = h->sc_host->steps;
+  if ((rc = ensure_graph(h))) return rc;
+  const int chunk = 64;
+  int done = 0;
+  while (done < max_steps) {
+    const int n = std::min(chunk, max_steps - done);
+    for (int k = 0; k < n; ++k) {
+      CK(cudaGraphLaunch(h->graph, h->st));
+      h->launches += h->step_launches;
+    }
+    done += n;
+    if ((rc = sync_scal(h))) return rc;
+    if (h->sc_host->status) break;
+    if (!(h->sc_host->t < tend)) break;
+  }
+  if ((rc = sync_scal(h))) return rc;
+  *t = h->sc_host->t;
+  if (steps) *steps = (int32_t)(h->sc_host->steps - s0);
+  if (h->sc_host->status) return fail(GDF_ERR_NUMERIC, "non-finite or non-positive state or dt during advance");
+  return GDF_OK;
+}
+
+int gdf_set_device(int32_t device) {
+  CK(cudaSetDevice(device));
+  return GDF_OK;
+}
+
+int gdf_advance_timed(GdfHandle* h, double tend, int32_t steps, double* t, int32_t* taken, double* device_ms) {
+  if (!h || !t || !device_ms || steps < 1) return fail(GDF_ERR_ARG, "bad argument");
+  if (!h->uploaded) return fail(GDF_ERR_STATE, "no state uploaded");
+  int rc = set_scal(h, *t, tend, 1);
+  if (rc) return rc;
+  const long long s0 = h->sc_host->steps;
+  if ((rc = ensure_graph(h))) return rc;
+  if (!h->ev0) {
+    CK(cudaEventCreate(&h->ev0));
+    CK(cudaEventCreate(&h->ev1));
+  }
+  CK(cudaStreamSynchronize(h->st));
+  CK(cudaEventRecord(h->ev0, h->st));
+  for (int k = 0; k < steps; ++k) {
+    CK(cudaGraphLaunch(h->graph, h->st));
+    h->launches += h->step_launches;
+  }
+  CK(cudaEventRecord(h->ev1, h->st));
+  CK(cudaEventSynchronize(h->ev1));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+  *device_ms = ms;
+  if ((rc = sync_scal(h))) return rc;
+  *t = h->sc_host->t;
+  if (taken) *taken = (int32_t)(h->sc_host->steps - s0);
+  if (h->sc_host->status) return fail(GDF_ERR_NUMERIC, "non-finite or non-positive state or dt during advance");
+  return GDF_OK;
+}
+
+int gdf_lh(GdfHandle* h, const double* uh, double* du) {
+  if (!h || !uh || !du) return fail(GDF_ERR_ARG, "null argument");
+  int rc = check_dead_slots(h->cfg, uh);
+  if (rc) return rc;
+  const size_t ub = uh_bytes(h->cfg);
+  CK(cudaMemcpyAsync(h->UT, uh, ub, cudaMemcpyHostToDevice, h->st));
+  CK(cudaMemsetAsync(h->UI, 0, ub, h->st));  // du (ghost and dead entries stay 0)
+  if ((rc = launch_faces(h, h->UT, nullptr))) return rc;
+  rc = run_kernel(h, GDF_K_CELL, [&] {
+    k_cell<<<nblk(h->K.plane, CELL_BS), CELL_BS, 0, h->st>>>(h->K, h->UT, nullptr, nullptr, h->Fxh, h->Fyh, h->UI,
+                                                             nullptr, 0);
+  });
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(du, h->UI, ub, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return GDF_OK;
+}
+
+int gdf_lhez(GdfHandle* h, const double* uh, double* dez1, double* dez2) {
+  if (!h || !uh || !dez1 || !dez2) return fail(GDF_ERR_ARG, "null argument");
+  int rc = check_dead_slots(h->cfg, uh);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(h->UT, uh, uh_bytes(h->cfg), cudaMemcpyHostToDevice, h->st));
+  if ((rc = launch_faces(h, h->UT, nullptr))) return rc;
+  double *d1 = h->BX0, *d2 = h->BY0;
+  rc = run_kernel(h, GDF_K_BFACE, [&] {
+    k_bface<<<nblk(h->K.fxplane + h->K.fyplane, 128), 128, 0, h->st>>>(
+        h->K, h->EzRL, h->EzUD, h->EzV, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, d1, d2, nullptr, 0);
+  });
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(dez1, d1, bx_bytes(h->cfg), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaMemcpyAsync(dez2, d2, by_bytes(h->cfg), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return GDF_OK;
+}
+
+int gdf_limit(GdfHandle* h, double* uh, double* bx, double* by, int32_t* flags) {
+  if (!h || !uh || !bx || !by) return fail(GDF_ERR_ARG, "null argument");
+  int rc = check_dead_slots(h->cfg, uh);
+  if (rc) return rc;
+  const size_t ub = uh_bytes(h->cfg);
+  // the limiter works on the resident buffers; save and restore them
+  CK(cudaMemcpyAsync(h->UT, uh, ub, cudaMemcpyHostToDevice, h->st));
+  CK(cudaMemcpyAsync(h->U0, h->UT, ub, cudaMemcpyDeviceToDevice, h->st));
+  CK(cudaMemcpyAsync(h->BX0, bx, bx_bytes(h->cfg), cudaMemcpyHostToDevice, h->st));
+  CK(cudaMemcpyAsync(h->BY0, by, by_bytes(h->cfg), cudaMemcpyHostToDevice, h->st));
+  double* sBX = h->BX;
+  double* sBY = h->BY;
+  h->BX = h->BX0;
+  h->BY = h->BY0;
+  rc = launch_limit(h, h->UT, h->U0, 1, nullptr);
+  if (!rc) rc = launch_set_bc(h, h->U0, 1, nullptr);
+  h->BX = sBX;
+  h->BY = sBY;
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(uh, h->U0, ub, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaMemcpyAsync(bx, h->BX0, bx_bytes(h->cfg), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaMemcpyAsync(by, h->BY0, by_bytes(h->cfg), cudaMemcpyDeviceToHost, h->st));
+  if (flags)
+    CK(cudaMemcpyAsync(flags, h->flags, (size_t)h->cfg.nx * h->cfg.ny * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                       h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return GDF_OK;
+}
+
+int gdf_dt(GdfHandle* h, const double* uh, double* dt) {
+  if (!h || !uh || !dt) return fail(GDF_ERR_ARG, "null argument");
+  CK(cudaMemcpyAsync(h->UT, uh, uh_bytes(h->cfg), cudaMemcpyHostToDevice, h->st));
+  int rc = launch_dt(h, h->UT, 0);
+  if (rc) return rc;
+  if ((rc = sync_scal(h))) return rc;
+  *dt = h->sc_host->dt;
+  return GDF_OK;
+}
+
+void* gdf_stream(GdfHandle* h) { return h ? (void*)h->st : nullptr; }
+
+int gdf_profile(GdfHandle* h, int32_t steps, double* ms_per_launch, int64_t* launches_per_kind, int32_t nkinds) {
+  if (!h || !ms_per_launch || steps < 1) return fail(GDF_ERR_ARG, "bad argument");
+  if (!h->uploaded) return fail(GDF_ERR_STATE, "no state uploaded");
+  if (!h->ev0) {
+    CK(cudaEventCreate(&h->ev0));
+    CK(cudaEventCreate(&h->ev1));
+  }
+  for (int k = 0; k < GDF_KERNEL_KINDS; ++k) { h->prof_ms[k] = 0; h->prof_n[k] = 0; }
+  int rc = sync_scal(h);
+  if (rc) return rc;
+  const double t0 = h->sc_host->t;
+  if ((rc = set_scal(h, t0, 1e300, 1))) return rc;
+  h->prof = 1;
+  for (int s = 0; s < steps && !rc; ++s) rc = launch_step(h);
+  h->prof = 0;
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(h->st));
+  for (int k = 0; k < nkinds && k < GDF_KERNEL_KINDS; ++k) {
+    ms_per_launch[k] = h->prof_n[k] ? h->prof_ms[k] / (double)h->prof_n[k] : 0.0;
+    if (launches_per_kind) launches_per_kind[k] = h->prof_n[k] / steps;
+  }
+  return GDF_OK;
+}
+
+int gdf_diagnostics(GdfHandle* h, double* umax, double* totaldiv, double* pmin, int64_t* n_troubled) {
+  if (!h) return fail(GDF_ERR_ARG, "null handle");
+  if (!h->uploaded) return fail(GDF_ERR_STATE, "no state uploaded");
+  const long long ncell = (long long)h->cfg.nx * h->cfg.ny;
+  const int nb = (int)nblk(ncell, DT_BS);
+  double* part = nullptr;
+  CK(cudaMallocAsync((void**)&part, (size_t)nb * 4 * sizeof(double), h->st));
+  int rc0 = run_kernel(h, GDF_K_DIAG, [&] { k_diag_partial<<<nb, DT_BS, 0, h->st>>>(h->K, h->U, h->flags, part); });
+  if (!rc0) rc0 = run_kernel(h, GDF_K_DIAG, [&] { k_diag_final<<<1, 32, 0, h->st>>>(h->K, part, nb, h->sc); });
+  if (rc0) return rc0;
+  CK(cudaFreeAsync(part, h->st));
+  int rc = sync_scal(h);
+  if (rc) return rc;
+  if (umax) *umax = h->sc_host->umax;
+  if (totaldiv) *totaldiv = h->sc_host->totaldiv;
+  if (pmin) *pmin = h->sc_host->pmin;
+  if (n_troubled) *n_troubled = h->sc_host->troubled;
+  return GDF_OK;
+}
+
+}  // extern "C"

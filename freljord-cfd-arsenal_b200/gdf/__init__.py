@@ -1,0 +1,231 @@
+"""Python host mirror of the reference's driver (main.f90 / RK3.f90) over the
+C ABI of include/gdf.h, for the B200 GDF P2 solver.
+
+The solver itself is the sm_100a library ``lib/libgdf_b200.so`` (or
+``lib/libgdf_b200_exact.so``, the FMA-free build); this module only binds
+it with ctypes. There is no CPU fallback: if the library is missing or no
+CUDA device is present, the constructors raise.
+
+Mapping to the reference (paths relative to GDF_Balsara_P2_0316/):
+  problem_config / init_data   init_data.f90 with an init*.txt problem
+  Solver.prepare               RK3.f90:5-12 (set_bc, TVB_Limiter_P2, div_free)
+  Solver.step                  one pass of the RK3.f90:58-174 loop body
+  Solver.advance               the RK3.f90 loop (device resident, graph)
+  Solver.lh / lhez / limit / dt  Lh, LhEz, TVB_Limiter_P2 + div_free_Balsara,
+                                 calculate_dt on caller arrays
+  Solver.diagnostics           calculate_umax / _totaldiv / _pmin
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from ._abi import (BC_OUTFLOW, BC_PERIODIC, DETECT_ALL, DETECT_KXRCF, FLUX_HLL, FLUX_HLLC, FLUX_HLLD,  # noqa: F401
+                   FLUX_LF, GDF_OK, LIB_DIR, NE, NP, PROB_BLAST, PROB_CLOUD_SHOCK, PROB_ORSZAG_TANG,
+                   PROB_ROTOR, PROB_VORTEX, GdfConfig, bx_shape, by_shape, dptr, iptr, new_state,
+                   problem_config, reference_config, uh_shape)
+
+KERNEL_NAMES = ["set_bc", "face_x", "face_y", "vertex", "cell", "bface", "limit", "dt", "diag"]
+KERNEL_KINDS = len(KERNEL_NAMES)
+
+LIB_FAST = os.path.join(LIB_DIR, "libgdf_b200.so")
+LIB_EXACT = os.path.join(LIB_DIR, "libgdf_b200_exact.so")
+
+_libs: dict = {}
+
+
+class GdfError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"gdf error {code}: {msg}")
+        self.code = code
+
+
+def load(exact: bool = False):
+    """Load the sm_100a library (fast or exact build) and declare the ABI."""
+    path = LIB_EXACT if exact else LIB_FAST
+    if path in _libs:
+        return _libs[path]
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with freljord-cfd-arsenal_b200/build.py "
+                          "(the solver has no CPU fallback)")
+    L = C.CDLL(path)
+    vp, dp, ip, i32 = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int32), C.c_int32
+    cfgp = C.POINTER(GdfConfig)
+    L.gdf_last_error.restype = C.c_char_p
+    L.gdf_build_exact.restype = C.c_int
+    L.gdf_config_reference.argtypes = [i32, i32, cfgp]
+    L.gdf_problem_config.argtypes = [i32, i32, i32, cfgp, dp]
+    L.gdf_init_data.argtypes = [cfgp, i32, dp, dp, dp, dp]
+    L.gdf_create.argtypes = [cfgp, C.POINTER(vp)]
+    L.gdf_destroy.argtypes = [vp]
+    L.gdf_upload.argtypes = [vp, dp, dp, dp]
+    L.gdf_download.argtypes = [vp, dp, dp, dp]
+    L.gdf_prepare.argtypes = [vp, ip]
+    L.gdf_step.argtypes = [vp, C.c_double, dp, dp, ip]
+    L.gdf_advance.argtypes = [vp, C.c_double, i32, dp, ip]
+    L.gdf_lh.argtypes = [vp, dp, dp]
+    L.gdf_lhez.argtypes = [vp, dp, dp, dp]
+    L.gdf_limit.argtypes = [vp, dp, dp, dp, ip]
+    L.gdf_dt.argtypes = [vp, dp, dp]
+    L.gdf_diagnostics.argtypes = [vp, dp, dp, dp, C.POINTER(C.c_int64)]
+    L.gdf_get_time.argtypes = [vp, dp, dp]
+    L.gdf_set_time.argtypes = [vp, C.c_double]
+    L.gdf_kernel_launches.argtypes = [vp]
+    L.gdf_kernel_launches.restype = C.c_int64
+    L.gdf_stream.argtypes = [vp]
+    L.gdf_stream.restype = C.c_void_p
+    L.gdf_profile.argtypes = [vp, i32, dp, C.POINTER(C.c_int64), i32]
+    L.gdf_advance_timed.argtypes = [vp, C.c_double, i32, dp, ip, dp]
+    L.gdf_set_device.argtypes = [i32]
+    _libs[path] = L
+    return L
+
+
+def _check(L, rc: int) -> None:
+    if rc != GDF_OK:
+        raise GdfError(rc, L.gdf_last_error().decode())
+
+
+def set_device(device: int, exact: bool = False) -> None:
+    """gdf_set_device: the CUDA device this library uses on this thread."""
+    L = load(exact)
+    _check(L, L.gdf_set_device(device))
+
+
+def c_problem_config(problem: int, nx: int, ny: int, exact: bool = False):
+    """gdf_problem_config through the library (host-only call)."""
+    L = load(exact)
+    cfg = GdfConfig()
+    te = C.c_double()
+    _check(L, L.gdf_problem_config(problem, nx, ny, C.byref(cfg), C.byref(te)))
+    return cfg, te.value
+
+
+def init_data(cfg: GdfConfig, problem: int, params=None, exact: bool = False):
+    """init_data.f90 on the host: returns (uh, bx, by) in the reference layout."""
+    L = load(exact)
+    uh, bx, by = new_state(cfg.nx, cfg.ny)
+    p = None if params is None else dptr(np.ascontiguousarray(params, np.float64))
+    _check(L, L.gdf_init_data(C.byref(cfg), problem, p, dptr(uh), dptr(bx), dptr(by)))
+    return uh, bx, by
+
+
+class Solver:
+    """One device-resident GDF P2 problem (a gdf_create handle)."""
+
+    def __init__(self, cfg: GdfConfig, exact: bool = False):
+        self.L = load(exact)
+        self.cfg = cfg.copy()
+        self.nx, self.ny = cfg.nx, cfg.ny
+        h = C.c_void_p()
+        _check(self.L, self.L.gdf_create(C.byref(self.cfg), C.byref(h)))
+        self.h = h
+        self.t = 0.0
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.L.gdf_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _flags(self):
+        return np.zeros((self.ny, self.nx), np.int32)
+
+    def upload(self, uh, bx, by) -> None:
+        _check(self.L, self.L.gdf_upload(self.h, dptr(uh), dptr(bx), dptr(by)))
+
+    def download(self):
+        uh, bx, by = new_state(self.nx, self.ny)
+        _check(self.L, self.L.gdf_download(self.h, dptr(uh), dptr(bx), dptr(by)))
+        return uh, bx, by
+
+    def download_into(self, uh, bx, by) -> None:
+        """gdf_download into caller arrays (e.g. pinned host buffers)."""
+        _check(self.L, self.L.gdf_download(self.h, dptr(uh), dptr(bx), dptr(by)))
+
+    def prepare(self):
+        f = self._flags()
+        _check(self.L, self.L.gdf_prepare(self.h, iptr(f)))
+        self.t = 0.0
+        return f
+
+    def step(self, tend: float, flags: bool = True):
+        t = C.c_double(self.t)
+        dt = C.c_double()
+        f = self._flags() if flags else None
+        _check(self.L, self.L.gdf_step(self.h, tend, C.byref(t), C.byref(dt), iptr(f) if flags else None))
+        self.t = t.value
+        return t.value, dt.value, f
+
+    def advance(self, tend: float, max_steps: int):
+        t = C.c_double(self.t)
+        n = C.c_int32()
+        _check(self.L, self.L.gdf_advance(self.h, tend, max_steps, C.byref(t), C.byref(n)))
+        self.t = t.value
+        return t.value, n.value
+
+    def advance_timed(self, tend: float, steps: int):
+        """(t, steps taken, device ms) of `steps` graph replays."""
+        t = C.c_double(self.t)
+        n = C.c_int32()
+        ms = C.c_double()
+        _check(self.L, self.L.gdf_advance_timed(self.h, tend, steps, C.byref(t), C.byref(n), C.byref(ms)))
+        self.t = t.value
+        return t.value, n.value, ms.value
+
+    def lh(self, uh):
+        du = np.zeros_like(uh)
+        _check(self.L, self.L.gdf_lh(self.h, dptr(uh), dptr(du)))
+        return du
+
+    def lhez(self, uh):
+        _, d1, d2 = new_state(self.nx, self.ny)
+        _check(self.L, self.L.gdf_lhez(self.h, dptr(uh), dptr(d1), dptr(d2)))
+        return d1, d2
+
+    def limit(self, uh, bx, by):
+        f = self._flags()
+        _check(self.L, self.L.gdf_limit(self.h, dptr(uh), dptr(bx), dptr(by), iptr(f)))
+        return f
+
+    def dt(self, uh) -> float:
+        d = C.c_double()
+        _check(self.L, self.L.gdf_dt(self.h, dptr(uh), C.byref(d)))
+        return d.value
+
+    def diagnostics(self):
+        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        n = C.c_int64()
+        _check(self.L, self.L.gdf_diagnostics(self.h, C.byref(a), C.byref(b), C.byref(c), C.byref(n)))
+        return a.value, b.value, c.value, n.value
+
+    def time(self):
+        t, dt = C.c_double(), C.c_double()
+        _check(self.L, self.L.gdf_get_time(self.h, C.byref(t), C.byref(dt)))
+        return t.value, dt.value
+
+    def set_time(self, t: float) -> None:
+        _check(self.L, self.L.gdf_set_time(self.h, t))
+        self.t = t
+
+    def kernel_launches(self) -> int:
+        return self.L.gdf_kernel_launches(self.h)
+
+    def stream(self) -> int:
+        """The handle's cudaStream_t as an integer."""
+        return self.L.gdf_stream(self.h) or 0
+
+    def profile(self, steps: int = 1):
+        """Per kernel kind: (mean ms per launch, launches per step)."""
+        ms = np.zeros(KERNEL_KINDS)
+        n = np.zeros(KERNEL_KINDS, np.int64)
+        _check(self.L, self.L.gdf_profile(self.h, steps, dptr(ms), n.ctypes.data_as(C.POINTER(C.c_int64)),
+                                          KERNEL_KINDS))
+        return {KERNEL_NAMES[k]: (ms[k], int(n[k])) for k in range(KERNEL_KINDS)}

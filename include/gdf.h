@@ -1,0 +1,218 @@
+/*
+ * gdf.h - C ABI of the B200 (sm_100a) implementation of the 2-D ideal-MHD
+ * P2 discontinuous-Galerkin step with globally divergence-free (Balsara)
+ * constrained transport, as in GDF_Balsara_P2_0316/ of
+ * L1ssandra/Freljord-CFD-arsenal.
+ *
+ * The reference has no foreign-function interface: its "API" is a set of
+ * argument-less Fortran subroutines sharing COMMON blocks (com.txt:19-54),
+ * driven by main.f90:1-23 -> RK3.f90. Every entry point below replaces one
+ * of those subroutines (cited per function) and takes the reference's
+ * arrays in Fortran (column-major) order with the reference's extents, so
+ * a Fortran host can pass its COMMON arrays through iso_c_binding unchanged:
+ *
+ *   uh : real(8) uh(0:Nx+1, 0:Ny+1, 10, 8)
+ *        index  i + (Nx+2)*(j + (Ny+2)*((d-1) + 10*(n-1)))   (i,j from 0)
+ *   Bx : real(8) Bx(0:Nx, 1:Ny, 3)      index i + (Nx+1)*((j-1) + Ny*(d-1))
+ *   By : real(8) By(1:Nx, 0:Ny, 3)      index (i-1) + Nx*(j + (Ny+1)*(d-1))
+ *   du : same extents as uh; dEz1 as Bx; dEz2 as By.
+ *   flags : int32 flags(1:Nx, 1:Ny)     index (i-1) + Nx*(j-1)
+ *
+ * All arithmetic on the solver path is IEEE binary64. Every call returns an
+ * int status: GDF_OK (0) or a GDF_ERR_* code; gdf_last_error() gives the
+ * message of the last failure on the calling thread. Calls on one handle
+ * are not thread-safe; each handle owns its device memory and one CUDA
+ * stream, and every call is synchronous at return.
+ */
+#ifndef GDF_H
+#define GDF_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GDF_ABI_VERSION 1
+
+enum {
+  GDF_OK = 0,
+  GDF_ERR_ARG = 1,      /* bad argument or configuration                  */
+  GDF_ERR_CUDA = 2,     /* CUDA runtime failure (message has the detail)  */
+  GDF_ERR_NUMERIC = 3,  /* non-finite state or non-positive dt detected   */
+  GDF_ERR_TIMEOUT = 4,  /* a bounded device wait gave up                  */
+  GDF_ERR_NOMEM = 5,    /* device allocation failed                       */
+  GDF_ERR_STATE = 6     /* call out of order (e.g. step before upload)    */
+};
+
+/* Numerical flux (com.txt:1 flux_type; Lh.f90:220-230, LhEz.f90:57-65). */
+enum { GDF_FLUX_LF = 1, GDF_FLUX_HLL = 2, GDF_FLUX_HLLC = 3, GDF_FLUX_HLLD = 4 };
+
+/* Boundary conditions (set_bc.f90:5-27). */
+enum { GDF_BC_PERIODIC = 1, GDF_BC_OUTFLOW = 2 };
+
+/* Troubled-cell detector feeding the characteristic limiter
+ * (TVB_Limiter_P2.f90:12,22). */
+enum {
+  GDF_DETECT_ALL = 0,    /* reference as shipped: every cell is limited    */
+  GDF_DETECT_KXRCF = 1   /* KXRCF_Detector.f90 gates the limiter           */
+};
+
+/* Initial-data problems (init_data.f90:3-19 include list; sizes and
+ * parameters of the benchmark problems are set by the caller). */
+enum {
+  GDF_PROB_VORTEX = 0,      /* init1.txt smooth MHD vortex                 */
+  GDF_PROB_ORSZAG_TANG = 1, /* init3.txt                                   */
+  GDF_PROB_ROTOR = 2,       /* rotor, init4.txt / Rotor_functions.f90 shape */
+  GDF_PROB_BLAST = 3,       /* blast, init5.txt / p0.f90 shape             */
+  GDF_PROB_CLOUD_SHOCK = 4  /* init6.txt / Cloud_Shock_functions.f90       */
+};
+
+/*
+ * Run-time configuration. The reference fixes all of this at compile time
+ * (com.txt:1,7, init*.txt, calculate_dt.f90:5-9) or by commenting lines in
+ * and out; the knobs below name those lines. gdf_config_reference() fills
+ * the values of GDF_Balsara_P2_0316 as shipped.
+ */
+typedef struct GdfConfig {
+  int32_t nx, ny;            /* com.txt:1 Nx, Ny                               */
+  double xa, xb, ya, yb;     /* init*.txt domain                               */
+  int32_t bc_r, bc_l, bc_u, bc_d; /* init*.txt bcR/bcL/bcU/bcD                 */
+  double gamma;              /* com.txt:7 (Lh, eigenvalueMm, pressure)         */
+  double gamma_flux;         /* MHD_flux.f90:7 and eigenmatrix.f90:19 use 5/3
+                                whatever com.txt says; set equal to gamma for
+                                a consistent-gamma run                         */
+  int32_t flux_type;         /* GDF_FLUX_*                                      */
+  double cfl;                /* calculate_dt.f90:8 (0.15; DF 0.2)              */
+  double tvb_m;              /* init*.txt M (minmod.f90:10)                    */
+  double tvb_slope;          /* TVB_Limiter_P2.f90:111-112 factor (0.75; DF 2/3) */
+  double hlld_eps;           /* HLLD_Flux.f90:126 threshold (1e-4; DF 1e-12)   */
+  int32_t pp_limiter;        /* TVB_Limiter_P2.f90:123 call pp_Limiter         */
+  int32_t faceb_limiter;     /* TVB_Limiter_P2.f90:186-187 apply Bxmod/Bymod   */
+  int32_t ez_face_fhat;      /* LhEz.f90:6-31: 0 local LF Ez, 1 -Fxhat7/Fyhat6 */
+  int32_t eig_p_typo;        /* eigenmatrix.f90:21 DF form -0.5|u|^2           */
+  int32_t eig_identity;      /* eigenmatrix.f90:397-404 identity fallback      */
+  int32_t eig_y_zero_w;      /* DF TVB_Limiter_P2.f90:71 passes u3=B3=0        */
+  int32_t kml_w_term;        /* Lh.f90:126 KML includes w*B3 (DF drops it)     */
+  int32_t dt_floor_stop;     /* RK3.f90:69-71 dt<1e-7 ends the run             */
+  int32_t umax_all_vars;     /* DF calculate_umax over all 8 averages          */
+  int32_t detector;          /* GDF_DETECT_*                                    */
+  double kxrcf_ck;           /* KXRCF_Detector.f90:7 threshold Ck              */
+  int32_t kxrcf_sticky;      /* KXRCF flags never reset (Is_Trouble_Cell)      */
+  int32_t reserved_i[7];
+  double reserved_d[4];
+} GdfConfig;
+
+/* Reference configuration of GDF_Balsara_P2_0316 as shipped (HLL, CFL 0.15,
+ * gamma 5/3, M 10, no pp, no face-B limiting, every cell limited) on an
+ * nx x ny grid of [0,1]^2 with periodic boundaries. */
+int gdf_config_reference(int32_t nx, int32_t ny, GdfConfig *out);
+
+/* Problem presets: domain, boundaries, gamma, M and flux of the named
+ * problem on an nx x ny grid, over the reference configuration. Replaces
+ * the init*.txt include (init_data.f90:19). *tend receives the end time. */
+int gdf_problem_config(int32_t problem, int32_t nx, int32_t ny, GdfConfig *out,
+                       double *tend);
+
+/* Host-side initial data (init_data.f90:1-123: L2 projection of cells and
+ * faces, or point values when the problem is a shock problem). params may
+ * be NULL for the defaults; for GDF_PROB_BLAST it is
+ * {cx, cy, r0, p_in, p_out, rho, Bx, By}. Writes uh (ghosts zero), Bx, By.
+ * Pure host code; no device is touched. */
+int gdf_init_data(const GdfConfig *cfg, int32_t problem, const double *params,
+                  double *uh, double *bx, double *by);
+
+typedef struct GdfHandle GdfHandle;
+
+/* Allocate device state for cfg on the current CUDA device. */
+int gdf_create(const GdfConfig *cfg, GdfHandle **out);
+int gdf_destroy(GdfHandle *h);
+
+/* Copy the full reference arrays to / from the device (synchronous). */
+int gdf_upload(GdfHandle *h, const double *uh, const double *bx, const double *by);
+int gdf_download(GdfHandle *h, double *uh, double *bx, double *by);
+
+/* RK3.f90:5-12: t = 0, set_bc, TVB_Limiter_P2, div_free_Balsara on the
+ * resident state. flags (may be NULL) receives the troubled-cell word of
+ * that limiter pass (bits 0-7 changed variables, bit 24 KXRCF flag). */
+int gdf_prepare(GdfHandle *h, int32_t *flags);
+
+/* One SSP-RK3 step of the resident state: RK3.f90:60-151 (calculate_dt,
+ * t clamp, 3 x [set_bc, Lh, LhEz, combine, TVB_Limiter_P2,
+ * div_free_Balsara]). *t is read as the current time and receives the new
+ * time; *dt_out receives dt. flags (may be NULL) receives per cell the
+ * changed-variable masks of stage 1/2/3 in bits 0-7/8-15/16-23 and the
+ * KXRCF flags of the three stages in bits 24/25/26. */
+int gdf_step(GdfHandle *h, double tend, double *t, double *dt_out, int32_t *flags);
+
+/* Up to max_steps steps (device-resident loop, no host sync between
+ * steps); stops once t reaches tend. *steps receives the number taken. */
+int gdf_advance(GdfHandle *h, double tend, int32_t max_steps, double *t,
+                int32_t *steps);
+
+/* gdf_advance without intermediate host synchronisation, with the device
+ * time of the `steps` graph replays (CUDA events on the handle's stream,
+ * recorded before the first and after the last) in *device_ms. */
+int gdf_advance_timed(GdfHandle *h, double tend, int32_t steps, double *t,
+                      int32_t *steps_taken, double *device_ms);
+
+/* Make `device` the current CUDA device of the calling thread for this
+ * library (one process per GPU; call before gdf_create). */
+int gdf_set_device(int32_t device);
+
+/* Fine-grained drop-ins on caller arrays (uploaded, computed, downloaded).
+ * gdf_lh:   Lh.f90 (du for all cells; ghost entries 0). uh ghosts are used
+ *           as given, as Lh does.
+ * gdf_lhez: LhEz.f90 (dEz1, dEz2) for the same uh, Bx, By.
+ * gdf_limit: TVB_Limiter_P2.f90 then div_free_Balsara.f90 on uh (ghosts as
+ *           given, rewritten by its set_bc), Bx, By in place.
+ * gdf_dt:   calculate_dt.f90 on the cell averages of uh.                 */
+int gdf_lh(GdfHandle *h, const double *uh, double *du);
+int gdf_lhez(GdfHandle *h, const double *uh, double *dez1, double *dez2);
+int gdf_limit(GdfHandle *h, double *uh, double *bx, double *by, int32_t *flags);
+int gdf_dt(GdfHandle *h, const double *uh, double *dt);
+
+/* calculate_umax.f90, calculate_totaldiv.f90, calculate_pmin.f90 on the
+ * resident state, plus the number of cells flagged by the last step. */
+int gdf_diagnostics(GdfHandle *h, double *umax, double *totaldiv, double *pmin,
+                    int64_t *n_troubled);
+
+/* Time and dt of the resident state (RK3.f90 t, dt). */
+int gdf_get_time(GdfHandle *h, double *t, double *dt);
+int gdf_set_time(GdfHandle *h, double t);
+
+/* Number of kernels this handle has launched since creation. */
+int64_t gdf_kernel_launches(GdfHandle *h);
+
+/* The handle's CUDA stream (a cudaStream_t), for callers that time or
+ * order work against it. No counterpart in the reference. */
+void *gdf_stream(GdfHandle *h);
+
+/* Kernel kinds reported by gdf_profile. */
+enum {
+  GDF_K_SET_BC = 0, GDF_K_FACE_X = 1, GDF_K_FACE_Y = 2, GDF_K_VERTEX = 3,
+  GDF_K_CELL = 4, GDF_K_BFACE = 5, GDF_K_LIMIT = 6, GDF_K_DT = 7, GDF_K_DIAG = 8,
+  GDF_KERNEL_KINDS = 9
+};
+
+/* Run `steps` time steps of the resident state with CUDA events around
+ * every launch (serialised, not graph-captured) and return, per kernel
+ * kind, the mean device time of one launch in ms and the launches of that
+ * kind per step. The reference times nothing (its SYSTEM_CLOCK calls in
+ * TVB_Limiter_P2.f90:10,14,189 are commented out); this is the
+ * per-kernel tracing of the port. */
+int gdf_profile(GdfHandle *h, int32_t steps, double *ms_per_launch,
+                int64_t *launches_per_kind, int32_t nkinds);
+
+/* Message of the last failure on this thread ("" if none). */
+const char *gdf_last_error(void);
+
+/* 1 when the library was built without FMA contraction (bit-faithful to
+ * an FMA-free CPU build of the reference), 0 for the fast build. */
+int gdf_build_exact(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GDF_H */

@@ -1,0 +1,325 @@
+"""Parity of the sm_100a library with the CPU oracle, through the C ABI.
+
+Two builds are checked:
+  exact  (libgdf_b200_exact.so, --fmad=false): every array equals the
+         oracle's value for value (== comparison, so -0 == +0);
+  fast   (libgdf_b200.so, FMA contraction): relative L1 per variable per
+         step <= 1e-12, with identical troubled-cell flag sets.
+Per-step parity is taken along the oracle's trajectory: both sides advance
+the same input state by one step. Sizes are those the oracle finishes in
+seconds; the full benchmark sizes are covered by size-independent
+properties at the end."""
+import numpy as np
+import pytest
+
+import gdf
+from oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12   # relative L1 per variable per step (fast build)
+
+CASES = {
+    "ot": (gdf.PROB_ORSZAG_TANG, 24, 16),
+    "rotor": (gdf.PROB_ROTOR, 20, 20),
+    "blast": (gdf.PROB_BLAST, 16, 18),
+    "cloud": (gdf.PROB_CLOUD_SHOCK, 24, 12),
+    "vortex": (gdf.PROB_VORTEX, 16, 16),
+}
+
+
+def setup(case, edit=None):
+    problem, nx, ny = CASES[case]
+    cfg, _ = gdf.problem_config(problem, nx, ny)
+    if edit:
+        edit(cfg)
+    o = Oracle(cfg)
+    uh, bx, by = o.init_data(problem)
+    return cfg, o, uh, bx, by
+
+
+def equal(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return bool(np.all((a == b) | (np.isnan(a) & np.isnan(b))))
+
+
+def rel_l1_uh(a, b):
+    """Relative L1 per variable over interior cells and all modes; variables
+    whose reference sum is zero are measured against the density sum."""
+    d = np.abs(a - b)[:, :, 1:-1, 1:-1].sum(axis=(1, 2, 3))
+    s = np.abs(b)[:, :, 1:-1, 1:-1].sum(axis=(1, 2, 3))
+    s = np.where(s > 0, s, s[0])
+    return d / s
+
+
+def rel_l1(a, b):
+    s = np.abs(b).sum()
+    return np.abs(a - b).sum() / (s if s > 0 else 1.0)
+
+
+def check(a, b, exact, what):
+    if exact:
+        bad = ~((a == b) | (np.isnan(a) & np.isnan(b)))
+        assert not bad.any(), f"{what}: {bad.sum()} entries differ, e.g. {np.argwhere(bad)[:3]}"
+    else:
+        r = rel_l1_uh(a, b) if a.ndim == 4 else np.array([rel_l1(a, b)])
+        assert (r <= TOL).all(), f"{what}: relative L1 {r}"
+
+
+@pytest.mark.parametrize("exact", [True, False], ids=["exact", "fast"])
+@pytest.mark.parametrize("case", list(CASES))
+def test_lh_lhez_dt(case, exact):
+    cfg, o, uh, bx, by = setup(case)
+    o.prepare(uh, bx, by)
+    o.set_bc(uh)
+    s = gdf.Solver(cfg, exact=exact)
+    check(s.lh(uh), o.lh(uh), exact, "Lh du")
+    d1, d2 = s.lhez(uh)
+    e1, e2 = o.lhez(uh)
+    check(d1, e1, exact, "LhEz dEz1")
+    check(d2, e2, exact, "LhEz dEz2")
+    dt = s.dt(uh)
+    assert dt == o.dt(uh) if exact else abs(dt - o.dt(uh)) <= 1e-14 * dt
+
+
+@pytest.mark.parametrize("exact", [True, False], ids=["exact", "fast"])
+@pytest.mark.parametrize("case", list(CASES))
+def test_limit(case, exact):
+    cfg, o, uh, bx, by = setup(case)
+    o.set_bc(uh)
+    # perturb into a state the limiter acts on: one forward-Euler stage
+    du = o.lh(uh)
+    d1, d2 = o.lhez(uh)
+    dt = o.dt(uh)
+    uh = uh + dt * du
+    bx, by = bx + dt * d1, by + dt * d2
+    ua, ba, ca = uh.copy(), bx.copy(), by.copy()
+    fo = o.limit(uh, bx, by)
+    s = gdf.Solver(cfg, exact=exact)
+    fs = s.limit(ua, ba, ca)
+    check(ua, uh, exact, "limited uh")
+    check(ba, bx, exact, "Bx")
+    check(ca, by, exact, "By")
+    assert np.array_equal(fs != 0, fo != 0), "troubled-cell sets differ"
+    if exact:
+        assert np.array_equal(fs, fo)
+
+
+@pytest.mark.parametrize("exact", [True, False], ids=["exact", "fast"])
+@pytest.mark.parametrize("case", list(CASES))
+def test_prepare_and_steps_along_oracle_trajectory(case, exact):
+    cfg, o, uh, bx, by = setup(case)
+    s = gdf.Solver(cfg, exact=exact)
+    s.upload(uh, bx, by)
+    fs = s.prepare()
+    fo = o.prepare(uh, bx, by)
+    u2, b2, c2 = s.download()
+    check(u2, uh, exact, "prepare uh")
+    assert np.array_equal(fs != 0, fo != 0)
+    t = 0.0
+    for k in range(4):
+        s.upload(uh, bx, by)
+        s.t = t
+        tg, dtg, fg = s.step(1e9)
+        to, dto, fo = o.step(uh, bx, by, t, 1e9)
+        ug, bxg, byg = s.download()
+        check(ug, uh, exact, f"step {k} uh")
+        check(bxg, bx, exact, f"step {k} Bx")
+        check(byg, by, exact, f"step {k} By")
+        assert (dtg == dto) if exact else abs(dtg - dto) <= 1e-13 * dto
+        assert np.array_equal(fg != 0, fo != 0), f"step {k}: troubled-cell sets differ"
+        if exact:
+            assert np.array_equal(fg, fo)
+        t = to
+
+
+@pytest.mark.parametrize("case", ["ot", "blast", "cloud"])
+def test_free_running_exact_build_stays_identical(case):
+    cfg, o, uh, bx, by = setup(case)
+    s = gdf.Solver(cfg, exact=True)
+    s.upload(uh, bx, by)
+    s.prepare()
+    o.prepare(uh, bx, by)
+    t = 0.0
+    for _ in range(6):
+        s.step(1e9)
+        t, _, _ = o.step(uh, bx, by, t, 1e9)
+    ug, bxg, byg = s.download()
+    assert equal(ug, uh) and equal(bxg, bx) and equal(byg, by)
+
+
+def _df(cfg):       # MHD_Globally_Divergence_Free/ variant lines
+    cfg.cfl = 0.2
+    cfg.hlld_eps = 1e-12
+    cfg.tvb_slope = 2.0 / 3.0
+    cfg.pp_limiter = 1
+    cfg.faceb_limiter = 1
+    cfg.ez_face_fhat = 1
+    cfg.eig_p_typo = 1
+    cfg.eig_identity = 0
+    cfg.eig_y_zero_w = 1
+    cfg.kml_w_term = 0
+    cfg.dt_floor_stop = 0
+    cfg.umax_all_vars = 1
+
+
+VARIANTS = {
+    "df_hlld": lambda c: (_df(c), setattr(c, "flux_type", gdf.FLUX_HLLD)),
+    "df_hll": lambda c: (_df(c), setattr(c, "flux_type", gdf.FLUX_HLL)),
+    "hllc": lambda c: setattr(c, "flux_type", gdf.FLUX_HLLC),
+    "lf": lambda c: setattr(c, "flux_type", gdf.FLUX_LF),
+    "kxrcf_nonsticky": lambda c: (setattr(c, "detector", gdf.DETECT_KXRCF), setattr(c, "kxrcf_ck", 0.5),
+                                  setattr(c, "kxrcf_sticky", 0)),
+    "consistent_gamma": lambda c: setattr(c, "gamma_flux", c.gamma),
+}
+
+
+@pytest.mark.parametrize("variant", list(VARIANTS))
+@pytest.mark.parametrize("case", ["cloud", "blast", "ot"])
+def test_variant_switches_exact(case, variant):
+    cfg, o, uh, bx, by = setup(case, VARIANTS[variant])
+    s = gdf.Solver(cfg, exact=True)
+    s.upload(uh, bx, by)
+    fs = s.prepare()
+    fo = o.prepare(uh, bx, by)
+    assert np.array_equal(fs, fo)
+    t = 0.0
+    for k in range(3):
+        _, _, fg = s.step(1e9)
+        t, _, fo = o.step(uh, bx, by, t, 1e9)
+        assert np.array_equal(fg, fo), f"step {k} flags"
+    ug, bxg, byg = s.download()
+    assert equal(ug, uh), np.argwhere(~((ug == uh) | np.isnan(uh)))[:4]
+    assert equal(bxg, bx) and equal(byg, by)
+
+
+@pytest.mark.parametrize("exact", [True, False], ids=["exact", "fast"])
+def test_advance_graph_matches_step_loop(exact):
+    cfg, o, uh, bx, by = setup("rotor")
+    a = gdf.Solver(cfg, exact=exact)
+    b = gdf.Solver(cfg, exact=exact)
+    for s in (a, b):
+        s.upload(uh, bx, by)
+        s.prepare()
+    for _ in range(5):
+        a.step(1e9, flags=False)
+    t, n = b.advance(1e9, 5)
+    assert n == 5 and t == a.t
+    for x, y in zip(a.download(), b.download()):
+        assert np.array_equal(x, y)
+
+
+def test_advance_stops_at_tend():
+    cfg, o, uh, bx, by = setup("ot")
+    s = gdf.Solver(cfg)
+    s.upload(uh, bx, by)
+    s.prepare()
+    t, n = s.advance(0.05, 1000)
+    assert t == 0.05 and 0 < n < 1000
+    t2, n2 = s.advance(0.05, 10)
+    assert n2 == 0 and t2 == 0.05
+
+
+def test_steps_are_deterministic():
+    cfg, o, uh, bx, by = setup("blast")
+    outs = []
+    for _ in range(2):
+        s = gdf.Solver(cfg)
+        s.upload(uh, bx, by)
+        s.prepare()
+        for _ in range(3):
+            s.step(1e9)
+        outs.append(s.download())
+    for x, y in zip(*outs):
+        assert np.array_equal(x, y)
+
+
+def test_diagnostics_match_oracle():
+    cfg, o, uh, bx, by = setup("rotor")
+    s = gdf.Solver(cfg, exact=True)
+    s.upload(uh, bx, by)
+    s.prepare()
+    o.prepare(uh, bx, by)
+    s.step(1e9)
+    o.step(uh, bx, by, 0.0, 1e9)
+    um, td, pm, nt = s.diagnostics()
+    um2, td2, pm2 = o.diagnostics(uh)
+    assert um == um2 and pm == pm2
+    assert td == pytest.approx(td2, rel=1e-10, abs=1e-15)
+
+
+def test_upload_rejects_dead_slots_and_bad_config():
+    cfg, o, uh, bx, by = setup("ot")
+    s = gdf.Solver(cfg)
+    bad = uh.copy()
+    bad[0, 8, 3, 3] = 1.0   # mode 9 of density is never populated by the P2 scheme
+    with pytest.raises(gdf.GdfError) as e:
+        s.upload(bad, bx, by)
+    assert e.value.code == gdf._abi.GDF_ERR_ARG
+    c2 = cfg.copy()
+    c2.flux_type = 7
+    with pytest.raises(gdf.GdfError):
+        gdf.Solver(c2)
+    with pytest.raises(gdf.GdfError) as e:
+        gdf.Solver(cfg).step(1.0)
+    assert e.value.code == gdf._abi.GDF_ERR_STATE
+
+
+def test_numeric_status_reported():
+    cfg, o, uh, bx, by = setup("ot")
+    uh = uh.copy()
+    uh[0, 0, 5, 5] = -1.0          # negative density average
+    s = gdf.Solver(cfg)
+    s.upload(uh, bx, by)
+    with pytest.raises(gdf.GdfError) as e:
+        s.step(1e9)
+    assert e.value.code == gdf._abi.GDF_ERR_NUMERIC
+
+
+# ---------------------------------------------------------------- full size
+def _point_symmetry_residual(uh, sign_var):
+    inner = uh[:, :, 1:-1, 1:-1]
+    flip = inner[:, :, ::-1, ::-1]
+    sign_mode = np.array([1, -1, -1, 1, 1, 1, -1, -1, -1, -1])
+    exp = flip * sign_mode[None, :, None, None] * np.asarray(sign_var)[:, None, None, None]
+    return np.abs(inner - exp).max() / np.abs(inner).max()
+
+
+def test_rotor_512_step_properties():
+    problem = gdf.PROB_ROTOR
+    cfg, _ = gdf.problem_config(problem, 512, 512)
+    uh, bx, by = gdf.init_data(cfg, problem)
+    s = gdf.Solver(cfg)
+    s.upload(uh, bx, by)
+    s.prepare()
+    u0, _, _ = s.download()
+    m0 = u0[:, 0, 1:-1, 1:-1].sum(axis=(1, 2))
+    um, td0, pm, _ = s.diagnostics()
+    t, n = s.advance(1e9, 3)
+    u1, _, _ = s.download()
+    assert np.isfinite(u1).all()
+    m1 = u1[:, 0, 1:-1, 1:-1].sum(axis=(1, 2))
+    scale = np.abs(u0[:, 0, 1:-1, 1:-1]).sum(axis=(1, 2)).max()
+    assert np.abs(m1 - m0)[[0, 1, 2, 4]].max() < 1e-12 * scale      # periodic conservation
+    _, td, _, _ = s.diagnostics()
+    assert td < 1e-10                                                # divergence-free
+    # the rotor is symmetric under rotation by pi about the centre:
+    # rho, E even; momenta odd; B even (uniform Bx background)
+    assert _point_symmetry_residual(u1, [1, -1, -1, -1, 1, 1, 1, 1]) < 1e-9
+
+
+def test_blast_2048_step_properties():
+    problem = gdf.PROB_BLAST
+    cfg, _ = gdf.problem_config(problem, 2048, 2048)
+    uh, bx, by = gdf.init_data(cfg, problem)
+    s = gdf.Solver(cfg)
+    s.upload(uh, bx, by)
+    s.prepare()
+    t, n = s.advance(1e9, 2)
+    assert n == 2
+    u1, _, _ = s.download()
+    assert np.isfinite(u1).all()
+    _, td, _, nt = s.diagnostics()
+    assert td < 1e-8
+    assert nt > 0
+    assert _point_symmetry_residual(u1, [1, -1, -1, -1, 1, 1, 1, 1]) < 1e-9
