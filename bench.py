@@ -185,6 +185,22 @@ def run_reference(args):
     return 0
 
 
+def run_quick(args):
+    """Warm-up and timed steps only: the command the ncu captures run."""
+    import gdf
+    gdf.set_device(dist_env()[2])
+    cfg, uh, bx, by = make_state(gdf)
+    s = gdf.Solver(cfg, exact=not args.fma)
+    s.upload(uh, bx, by)
+    s.prepare()
+    if args.warmup:
+        s.advance_timed(1e9, args.warmup)
+    _, n, ms = s.advance_timed(1e9, args.steps)
+    print(json.dumps({"quick": True, "steps": n, "ms_per_step": ms / n, "value": NX * NY * n / (ms / 1e3)}))
+    s.close()
+    return 0
+
+
 def run_ours(args):
     world, rank, local = dist_env()
     import numpy as np
@@ -254,6 +270,18 @@ def run_ours(args):
     e2e = world * NX * NY * e2e_steps / e2e_el
     io_bytes = huh.nbytes + hbx.nbytes + hby.nbytes
 
+    # the opt-in FMA build on the same workload, for comparison
+    fma = None
+    if not args.no_fma:
+        f = gdf.Solver(cfg, exact=False)
+        f.upload(uh, bx, by)
+        f.prepare()
+        f.advance_timed(1e9, 3)
+        _, _, fms = f.advance_timed(1e9, args.steps)
+        fma = {"value": NX * NY * args.steps / (fms / 1e3), "unit": UNIT, "ms_per_step": fms / args.steps,
+               "build": "libgdf_b200_fma.so (FMA contraction; not tie-exact)"}
+        f.close()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(gdf, args.cpu_steps)
@@ -276,6 +304,8 @@ def run_ours(args):
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(io_bytes),
                     "d2h_bytes_per_step": int(io_bytes), "steps": e2e_steps},
             "cpu_baseline": cpu,
+            "fma_build": fma,
+            "build": "libgdf_b200.so (no FMA contraction: value-exact with the reference arithmetic)",
             "clocks": clocks,
             "steps_taken": taken,
         }
@@ -295,7 +325,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--no-fma", action="store_true")
+    ap.add_argument("--quick", action="store_true", help="timed steps only (for profiler captures)")
+    ap.add_argument("--fma", action="store_true", help="with --quick: run the FMA build")
     args = ap.parse_args()
+    if args.quick:
+        return run_quick(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

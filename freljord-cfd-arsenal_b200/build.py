@@ -1,9 +1,12 @@
 """Build the sm_100a shared libraries of the GDF P2 step, in-tree.
 
 Produces, under freljord-cfd-arsenal_b200/lib/:
-  libgdf_b200.so        the product build (FMA contraction on)
-  libgdf_b200_exact.so  the same sources with --fmad=false, whose arithmetic
-                        follows an FMA-free CPU build of the reference
+  libgdf_b200.so        the product build: --fmad=false, so every FP64
+                        operation rounds as in an FMA-free CPU build of the
+                        reference (bit-faithful step, identical flag sets)
+  libgdf_b200_fma.so    the same sources with FMA contraction on (faster
+                        arithmetic; results differ in the last bits and can
+                        flip a limiter decision that sits on a threshold)
 Both export the C ABI of include/gdf.h. Rebuilds only what is out of date.
 """
 from __future__ import annotations
@@ -58,8 +61,8 @@ def build(verbose: bool = False) -> dict:
         _run([HOST_CXX, "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-march=x86-64",
               "-c", HOST_SRC, "-o", host_o])
     out = {}
-    for name, flags in (("libgdf_b200.so", ["--fmad=true"]),
-                        ("libgdf_b200_exact.so", ["--fmad=false", "-DGDF_EXACT=1"])):
+    for name, flags in (("libgdf_b200.so", ["--fmad=false", "-DGDF_EXACT=1"]),
+                        ("libgdf_b200_fma.so", ["--fmad=true"])):
         obj = os.path.join(BUILD, name.replace(".so", ".o"))
         so = os.path.join(LIB, name)
         if _stale(obj, [KERNEL_SRC] + HEADERS):

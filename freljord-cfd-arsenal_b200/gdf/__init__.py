@@ -1,9 +1,10 @@
 """Python host mirror of the reference's driver (main.f90 / RK3.f90) over the
 C ABI of include/gdf.h, for the B200 GDF P2 solver.
 
-The solver itself is the sm_100a library ``lib/libgdf_b200.so`` (or
-``lib/libgdf_b200_exact.so``, the FMA-free build); this module only binds
-it with ctypes. There is no CPU fallback: if the library is missing or no
+The solver itself is the sm_100a library ``lib/libgdf_b200.so`` (built
+without FMA contraction, so its arithmetic follows the reference's) or, on
+request, ``lib/libgdf_b200_fma.so`` (FMA contraction on); this module only
+binds it with ctypes. There is no CPU fallback: if the library is missing or no
 CUDA device is present, the constructors raise.
 
 Mapping to the reference (paths relative to GDF_Balsara_P2_0316/):
@@ -30,8 +31,9 @@ from ._abi import (BC_OUTFLOW, BC_PERIODIC, DETECT_ALL, DETECT_KXRCF, FLUX_HLL, 
 KERNEL_NAMES = ["set_bc", "face_x", "face_y", "vertex", "cell", "bface", "limit", "dt", "diag"]
 KERNEL_KINDS = len(KERNEL_NAMES)
 
-LIB_FAST = os.path.join(LIB_DIR, "libgdf_b200.so")
-LIB_EXACT = os.path.join(LIB_DIR, "libgdf_b200_exact.so")
+LIB_EXACT = os.path.join(LIB_DIR, "libgdf_b200.so")
+LIB_FMA = os.path.join(LIB_DIR, "libgdf_b200_fma.so")
+LIB_FAST = LIB_FMA
 
 _libs: dict = {}
 
@@ -42,9 +44,10 @@ class GdfError(RuntimeError):
         self.code = code
 
 
-def load(exact: bool = False):
-    """Load the sm_100a library (fast or exact build) and declare the ABI."""
-    path = LIB_EXACT if exact else LIB_FAST
+def load(exact: bool = True):
+    """Load the sm_100a library (the product build, or the FMA build when
+    exact is False) and declare the ABI."""
+    path = LIB_EXACT if exact else LIB_FMA
     if path in _libs:
         return _libs[path]
     if not os.path.exists(path):
@@ -88,13 +91,13 @@ def _check(L, rc: int) -> None:
         raise GdfError(rc, L.gdf_last_error().decode())
 
 
-def set_device(device: int, exact: bool = False) -> None:
+def set_device(device: int, exact: bool = True) -> None:
     """gdf_set_device: the CUDA device this library uses on this thread."""
     L = load(exact)
     _check(L, L.gdf_set_device(device))
 
 
-def c_problem_config(problem: int, nx: int, ny: int, exact: bool = False):
+def c_problem_config(problem: int, nx: int, ny: int, exact: bool = True):
     """gdf_problem_config through the library (host-only call)."""
     L = load(exact)
     cfg = GdfConfig()
@@ -103,7 +106,7 @@ def c_problem_config(problem: int, nx: int, ny: int, exact: bool = False):
     return cfg, te.value
 
 
-def init_data(cfg: GdfConfig, problem: int, params=None, exact: bool = False):
+def init_data(cfg: GdfConfig, problem: int, params=None, exact: bool = True):
     """init_data.f90 on the host: returns (uh, bx, by) in the reference layout."""
     L = load(exact)
     uh, bx, by = new_state(cfg.nx, cfg.ny)
@@ -115,7 +118,7 @@ def init_data(cfg: GdfConfig, problem: int, params=None, exact: bool = False):
 class Solver:
     """One device-resident GDF P2 problem (a gdf_create handle)."""
 
-    def __init__(self, cfg: GdfConfig, exact: bool = False):
+    def __init__(self, cfg: GdfConfig, exact: bool = True):
         self.L = load(exact)
         self.cfg = cfg.copy()
         self.nx, self.ny = cfg.nx, cfg.ny

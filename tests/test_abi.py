@@ -27,7 +27,7 @@ def declared_symbols():
 
 @pytest.mark.parametrize("exact", [False, True])
 def test_every_declared_symbol_is_exported(exact):
-    lib = gdf.LIB_EXACT if exact else gdf.LIB_FAST
+    lib = gdf.LIB_EXACT if exact else gdf.LIB_FMA
     out = subprocess.run(["nm", "-D", "--defined-only", lib], capture_output=True, text=True, check=True).stdout
     exported = set(re.findall(r" T (gdf_\w+)", out))
     syms = declared_symbols()
