@@ -123,6 +123,21 @@ def dist_env():
     return world, rank, local
 
 
+def reduce_max_ms(ms: float, dist, device) -> float:
+    """Max over ranks of the device-timed region (ms); identity on one rank."""
+    if dist is None:
+        return ms
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(world: int, steps: int, ms_max: float) -> float:
+    """Whole-job cell-updates/s: every rank advances its own replica."""
+    return world * NX * NY * steps / (ms_max / 1e3)
+
+
 def make_state(gdf):
     cfg, _ = gdf.problem_config(gdf.PROB_ROTOR, NX, NY)
     uh, bx, by = gdf.init_data(cfg, gdf.PROB_ROTOR)
@@ -227,13 +242,8 @@ def run_ours(args):
     _, taken, ms = s.advance_timed(1e9, args.steps)
     launches = s.kernel_launches() - l0
     clocks = clk.stop()
-    ms_max = ms
-    if dist:
-        import torch
-        tt = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms_max = float(tt.item())
-    value = world * NX * NY * args.steps / (ms_max / 1e3)
+    ms_max = reduce_max_ms(ms, dist, f"cuda:{local}")
+    value = job_value(world, args.steps, ms_max)
 
     # per-kernel timing (events around every launch) for the roofline
     prof = s.profile(2)

@@ -1,0 +1,57 @@
+"""bench.py's multi-GPU path is replicas only: each rank advances its own
+copy of the workload and the job time is the max over ranks. The rank
+logic runs here on CPU with the gloo backend, world size 2."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, REPO)
+
+
+def _worker(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    import datetime
+    import bench
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    ms = 10.0 + 5.0 * rank          # rank 1 is the slow one
+    m = bench.reduce_max_ms(ms, dist, "cpu")
+    v = bench.job_value(world, 4, m)
+    dist.barrier()
+    dist.destroy_process_group()
+    q.put((rank, m, v))
+
+
+def test_max_over_ranks_and_job_value():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 29500 + os.getpid() % 1000
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    res = sorted(q.get(timeout=10) for _ in range(2))
+    import bench
+    for rank, m, v in res:
+        assert m == 15.0
+        assert v == pytest.approx(2 * bench.NX * bench.NY * 4 / 0.015)
+
+
+def test_reference_arm_nonzero_rank_exits_quietly():
+    env = dict(os.environ, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
+    r = subprocess.run([sys.executable, os.path.join(REPO, "bench.py"), "--impl", "reference", "--gpus", "2",
+                        "--steps", "1", "--warmup", "0"], capture_output=True, text=True, env=env, timeout=120)
+    assert r.returncode == 0
+    assert r.stdout.strip() == ""
+
+
+def test_single_rank_reduce_is_identity():
+    import bench
+    assert bench.reduce_max_ms(3.5, None, "cpu") == 3.5
