@@ -26,6 +26,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1250,6 +1251,21 @@ static int check_dead_slots(const GdfConfig& c, const double* uh) {
   return GDF_OK;
 }
 
+// ------------------------------------------------------------------------
+// Scratch of gdf_lh_noalloc: the face fluxes (Fxhat, Fyhat) and face Ez that
+// k_face writes and k_cell reads, for grids with at most NOALLOC_MAX_FACES
+// faces per direction. The module holds this array on every device that
+// loads the library, until the process exits. Host code must not use the
+// symbol as a device address; gdf_lh_noalloc takes its address per device
+// with cudaGetSymbolAddress.
+constexpr long long NOALLOC_MAX_FACES = 16640;  // (nx+1)*ny and nx*(ny+1); 128 x 128 fits
+constexpr long long NOALLOC_DOUBLES = 2 * NOALLOC_MAX_FACES * (NG * NE + NG);
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_DOUBLES];
+
+constexpr int NOALLOC_MAX_DEVICES = 256;
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_addr[NOALLOC_MAX_DEVICES] = {nullptr};
+
 // Capture one time step (RK3.f90:60-151) of the resident state as a CUDA
 // graph; replays need no host work between steps.
 static int ensure_graph(GdfHandle* h) {
@@ -1466,6 +1482,54 @@ int gdf_advance(GdfHandle* h, double tend, int32_t max_steps, double* t, int32_t
   *t = h->sc_host->t;
   if (steps) *steps = (int32_t)(h->sc_host->steps - s0);
   if (h->sc_host->status) return fail(GDF_ERR_NUMERIC, "non-finite or non-positive state or dt during advance");
+  return GDF_OK;
+}
+
+// Lh of one grid on caller-owned device buffers, allocating nothing (the
+// face-flux scratch is g_noalloc_scratch). Stream-ordered on `stream`;
+// returns after enqueueing.
+int gdf_lh_noalloc(const GdfConfig* cfg, const double* d_uh, double* d_du, void* stream) {
+  int rc = check_config(cfg);
+  if (rc) return rc;
+  if (!d_uh || !d_du) return fail(GDF_ERR_ARG, "null device buffer");
+  const long long fx = (long long)(cfg->nx + 1) * cfg->ny, fy = (long long)cfg->nx * (cfg->ny + 1);
+  if (fx > NOALLOC_MAX_FACES || fy > NOALLOC_MAX_FACES)
+    return fail(GDF_ERR_ARG, "gdf_lh_noalloc: grid " + std::to_string(cfg->nx) + "x" + std::to_string(cfg->ny) +
+                                 " exceeds its fixed scratch: (nx+1)*ny and nx*(ny+1) must be at most " +
+                                 std::to_string(NOALLOC_MAX_FACES) + " (128x128 fits); use gdf_lh");
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(GDF_ERR_ARG, "device ordinal out of range");
+  void* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+      // first call on this device: resolve the device address of the
+      // scratch array with this device current
+      void* p = nullptr;
+      cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess)
+        return fail(GDF_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
+      g_noalloc_addr[dev] = p;
+    }
+    base = g_noalloc_addr[dev];
+  }
+  Consts K;
+  build_consts(*cfg, K);
+  double* Fxh = static_cast<double*>(base);
+  double* Fyh = Fxh + fx * NG * NE;
+  double* ezx = Fyh + fy * NG * NE;
+  double* ezy = ezx + fx * NG;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // every face point of Fxh/Fyh/Ez is written before k_cell reads it, so
+  // the scratch left by an earlier call needs no clearing; du's ghost and
+  // dead slots must read 0
+  CK(cudaMemsetAsync(d_du, 0, uh_bytes(*cfg), st));
+  k_face<0><<<nblk(fx * NG, 128), 128, 0, st>>>(K, d_uh, Fxh, ezx, nullptr);
+  k_face<1><<<nblk(fy * NG, 128), 128, 0, st>>>(K, d_uh, Fyh, ezy, nullptr);
+  k_cell<<<nblk(K.plane, CELL_BS), CELL_BS, 0, st>>>(K, d_uh, nullptr, nullptr, Fxh, Fyh, d_du, nullptr, 0);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(GDF_ERR_CUDA, std::string("gdf_lh_noalloc launch: ") + cudaGetErrorString(e));
   return GDF_OK;
 }
 

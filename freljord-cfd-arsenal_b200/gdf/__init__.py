@@ -82,6 +82,7 @@ def load(exact: bool = True):
     L.gdf_profile.argtypes = [vp, i32, dp, C.POINTER(C.c_int64), i32]
     L.gdf_advance_timed.argtypes = [vp, C.c_double, i32, dp, ip, dp]
     L.gdf_set_device.argtypes = [i32]
+    L.gdf_lh_noalloc.argtypes = [cfgp, vp, vp, vp]
     _libs[path] = L
     return L
 
@@ -95,6 +96,13 @@ def set_device(device: int, exact: bool = True) -> None:
     """gdf_set_device: the CUDA device this library uses on this thread."""
     L = load(exact)
     _check(L, L.gdf_set_device(device))
+
+
+def lh_noalloc(cfg: GdfConfig, d_uh: int, d_du: int, stream: int = 0, exact: bool = True) -> None:
+    """gdf_lh_noalloc: Lh on caller-owned device buffers (device pointers as
+    integers), enqueued on `stream`; allocates no device memory."""
+    L = load(exact)
+    _check(L, L.gdf_lh_noalloc(C.byref(cfg), C.c_void_p(d_uh), C.c_void_p(d_du), C.c_void_p(stream or None)))
 
 
 def c_problem_config(problem: int, nx: int, ny: int, exact: bool = True):

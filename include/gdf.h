@@ -172,6 +172,24 @@ int gdf_lhez(GdfHandle *h, const double *uh, double *dez1, double *dez2);
 int gdf_limit(GdfHandle *h, double *uh, double *bx, double *by, int32_t *flags);
 int gdf_dt(GdfHandle *h, const double *uh, double *dt);
 
+/* Lh (as gdf_lh) on caller-owned DEVICE buffers, allocating no device
+ * memory: d_uh and d_du are device pointers with the uh extents of the
+ * config (d_du receives du, ghost and unused entries 0). No counterpart in
+ * the reference. It is for callers that cannot call cudaMalloc: a host
+ * whose device memory is fully planned at start-up (the reference's
+ * static-COMMON model carried to the GPU), or code running inside a
+ * framework whose memory pool forbids allocations outside it. Its scratch
+ * (the face fluxes) is a fixed array compiled into this library, so every
+ * GPU that loads the library holds ~12 MB until the process exits, and the
+ * grid is limited to (nx+1)*ny <= 16640 and nx*(ny+1) <= 16640 faces
+ * (128 x 128 fits); larger grids get GDF_ERR_ARG. The first call on a
+ * device resolves the scratch's device address with that device current;
+ * make that first call before any stream capture. Work is enqueued on
+ * `stream` (a cudaStream_t, NULL for the default stream) and the call
+ * returns without synchronising. All calls share the one scratch array:
+ * calls that overlap on the GPU (other streams, other threads) race. */
+int gdf_lh_noalloc(const GdfConfig *cfg, const double *d_uh, double *d_du, void *stream);
+
 /* calculate_umax.f90, calculate_totaldiv.f90, calculate_pmin.f90 on the
  * resident state, plus the number of cells flagged by the last step. */
 int gdf_diagnostics(GdfHandle *h, double *umax, double *totaldiv, double *pmin,
