@@ -128,7 +128,11 @@ def test_limit(case, exact):
 @pytest.mark.parametrize("exact", [True, False], ids=["exact", "fma"])
 @pytest.mark.parametrize("case", list(CASES))
 def test_prepare_and_steps_along_oracle_trajectory(case, exact):
-    cfg, o, uh, bx, by = setup(case)
+    # Each step restarts from the oracle's state, but the sticky KXRCF flags
+    # live on both sides; for the FMA build a flag flipped at the threshold
+    # would persist, so that build runs with per-step (non-sticky) flags.
+    edit = None if exact else (lambda c: setattr(c, "kxrcf_sticky", 0))
+    cfg, o, uh, bx, by = setup(case, edit)
     s = gdf.Solver(cfg, exact=exact)
     s.upload(uh, bx, by)
     fs = s.prepare()
