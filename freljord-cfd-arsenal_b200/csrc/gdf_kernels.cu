@@ -52,6 +52,16 @@ __constant__ unsigned char c_live_d[NLIVE] = {0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5
                                               0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5,
                                               6, 8, 0, 1, 2, 3, 4, 5, 7, 9, 0, 1, 2, 3, 4, 5};
 
+// variable and mode of live slot s (the order of c_live_n / c_live_d)
+__host__ __device__ constexpr int slot_n(int s) { return s < 30 ? s / 6 : s < 38 ? 5 : s < 46 ? 6 : 7; }
+__host__ __device__ constexpr int slot_d(int s) {
+  return s < 30 ? s % 6 : s < 38 ? (s - 30 <= 6 ? s - 30 : 8) : s < 46 ? (s - 38 <= 5 ? s - 38 : (s == 44 ? 7 : 9)) : s - 46;
+}
+// structural zeros of the volume basis derivatives: phixG vanishes for
+// modes 1, 3, 6, 10 and phiyG for modes 1, 2, 4, 7 (get_basis.f90)
+__host__ __device__ constexpr bool px_zero(int d) { return d == 0 || d == 2 || d == 5 || d == 9; }
+__host__ __device__ constexpr bool py_zero(int d) { return d == 0 || d == 1 || d == 3 || d == 6; }
+
 __device__ __forceinline__ long long gtid() { return (long long)blockIdx.x * blockDim.x + threadIdx.x; }
 
 // ------------------------------------------------------------- set_bc ----
@@ -249,12 +259,23 @@ __global__ void __launch_bounds__(CELL_BS) k_cell(const __grid_constant__ Consts
         Fy[6] = 0.0;
         Fy[7] = vv * B3 - w * B2;
         const double coef = 0.25 * K.w[a] * K.w[b];
+        // du(d,n) += coef*(Fx*phixG + Fy*phiyG); a product with an exact zero
+        // (phixG of modes 1,3,6,10, phiyG of modes 1,2,4,7, Fx(6), Fy(7))
+        // contributes +-0 and is left out
 #pragma unroll
         for (int d = 1; d < NP; ++d)
 #pragma unroll
-          for (int n = 0; n < NE; ++n)
-            if (live_mode(n, d))
+          for (int n = 0; n < NE; ++n) {
+            if (!live_mode(n, d)) continue;
+            const bool hx = n != 5 && !px_zero(d);
+            const bool hy = n != 6 && !py_zero(d);
+            if (hx && hy)
               du[LI(n, d)] = du[LI(n, d)] + coef * (Fx[n] * K.phix[a][b][d] + Fy[n] * K.phiy[a][b][d]);
+            else if (hx)
+              du[LI(n, d)] = du[LI(n, d)] + coef * (Fx[n] * K.phix[a][b][d]);
+            else if (hy)
+              du[LI(n, d)] = du[LI(n, d)] + coef * (Fy[n] * K.phiy[a][b][d]);
+          }
       }
     }
     // surface terms in the reference order (x faces, then y faces), mass
@@ -274,10 +295,18 @@ __global__ void __launch_bounds__(CELL_BS) k_cell(const __grid_constant__ Consts
       for (int d = 0; d < NP; ++d) {
         if (!live_mode(n, d)) continue;
         double acc = du[LI(n, d)];
+        // at the middle point (lambda = 0) the face basis of modes 3, 5, 8,
+        // 10 (x faces) and 2, 5, 9, 7 (y faces) vanishes on both sides
 #pragma unroll
-        for (int g = 0; g < NG; ++g) acc = acc - K.cxs * K.w[g] * (fr[g] * K.phiGR[g][d] - fl[g] * K.phiGL[g][d]);
+        for (int g = 0; g < NG; ++g) {
+          if (g == 2 && (d == 2 || d == 4 || d == 7 || d == 9)) continue;
+          acc = acc - K.cxs * K.w[g] * (fr[g] * K.phiGR[g][d] - fl[g] * K.phiGL[g][d]);
+        }
 #pragma unroll
-        for (int g = 0; g < NG; ++g) acc = acc - K.cys * K.w[g] * (fu[g] * K.phiGU[g][d] - fd[g] * K.phiGD[g][d]);
+        for (int g = 0; g < NG; ++g) {
+          if (g == 2 && (d == 1 || d == 4 || d == 8 || d == 6)) continue;
+          acc = acc - K.cys * K.w[g] * (fu[g] * K.phiGU[g][d] - fd[g] * K.phiGD[g][d]);
+        }
         du[LI(n, d)] = acc / K.mm[d];
       }
     }
@@ -468,6 +497,12 @@ __device__ bool kxrcf_flag(const Consts& K, const double* __restrict__ S, long l
       Lij = Lij + K.hx;
     }
   }
+  // with every integral zero each ratio is exactly 0 (the denominator is
+  // positive), so the flag is decided without the point maxima
+  bool all_zero = true;
+#pragma unroll
+  for (int n = 0; n < NE; ++n) all_zero = all_zero && (I[n] == 0.0);
+  if (all_zero) return prev || (0.0 >= K.ck);
   double uinf[NE];
 #pragma unroll
   for (int n = 0; n < NE; ++n) uinf[n] = 0.0;
@@ -508,10 +543,29 @@ __device__ double pp_tq(const Consts& K, const double* ubar, const double* uq) {
 }
 
 // pp_Limiter.f90:10-81 for one cell's modes (in place)
+// Bound on |u_q - u_bar| over the 50 GLL-mixed points for variable n:
+// sum_d |m_d| max_q |phi_d(q)|, inflated to cover the rounding of the point
+// sums (relative error < 2.3e-15 of |u_bar| + the bound).
+__device__ __forceinline__ double pp_spread(const Consts& K, const double (*m)[NP], int n) {
+  double b = 0.0;
+#pragma unroll
+  for (int d = 1; d < NP; ++d)
+    if (live_mode(n, d)) b = b + fabs(m[n][d]) * K.ppM[d];
+  return b * (1.0 + 1e-12) + 1e-12 * fabs(m[n][0]);
+}
+
+// pp_Limiter.f90:10-81 for one cell's modes (in place). The density part
+// acts only if some point has |rho_bar - rho_q| > rho_bar - 1e-13, and the
+// pressure part only if some point has a negative pressure; when the
+// bounds of pp_spread rule that out (with margins far above rounding) the
+// point evaluations are skipped and the cell is left exactly as the full
+// evaluation would leave it.
 __device__ void pp_cell(const Consts& K, double (*m)[NP]) {
   const double epsilon = 1e-13;
   double eta = 1.0;
   const double rb = m[0][0];
+  const bool rho_safe = pp_spread(K, m, 0) < (rb - epsilon) * (1.0 - 1e-12);
+  if (!rho_safe) {
 #pragma unroll 1
   for (int a = 0; a < NG; ++a)
 #pragma unroll 1
@@ -529,6 +583,24 @@ __device__ void pp_cell(const Consts& K, double (*m)[NP]) {
     const double f = 0.5 * eta;
 #pragma unroll
     for (int d = 1; d < NP; ++d) m[0][d] = f * m[0][d];
+  }
+  }
+  {
+    // lower bound of the pressure at every point from bounds on the point
+    // values; a positive bound (beyond rounding) means no point has pq < 0
+    double dv[NE];
+#pragma unroll
+    for (int n = 0; n < NE; ++n) dv[n] = pp_spread(K, m, n);
+    const double rho_lo = m[0][0] - dv[0];
+    if (rho_lo > 0.0) {
+      const double e_lo = m[4][0] - dv[4];
+      const double k_hi = 0.5 * (sq(fabs(m[1][0]) + dv[1]) + sq(fabs(m[2][0]) + dv[2]) + sq(fabs(m[3][0]) + dv[3])) /
+                          rho_lo * (1.0 + 1e-12);
+      const double b_hi = 0.5 * (sq(fabs(m[5][0]) + dv[5]) + sq(fabs(m[6][0]) + dv[6]) + sq(fabs(m[7][0]) + dv[7])) *
+                          (1.0 + 1e-12);
+      const double p_lo = e_lo - k_hi - b_hi;
+      if (p_lo > 1e-10 * (fabs(e_lo) + k_hi + b_hi)) return;   // eta stays 1: nothing changes
+    }
   }
   double ubar[NE];
 #pragma unroll
@@ -592,7 +664,8 @@ __global__ void __launch_bounds__(LIM_BS) k_limit(const __grid_constant__ Consts
   bool gate = true;
   if (K.detector == GDF_DETECT_KXRCF) {
     const bool prev = K.sticky ? (trouble[item] != 0) : false;
-    gate = kxrcf_flag(K, S, c, m, prev);
+    // a set sticky flag stays set whatever the detector finds
+    gate = prev ? true : kxrcf_flag(K, S, c, m, prev);
     trouble[item] = gate ? 1 : 0;
     if (gate) word |= (1 << 24);
   }
@@ -1101,6 +1174,13 @@ static void build_consts(const GdfConfig& c, Consts& K) {
       X[8] = P2(lj) / hx1; Y[8] = 2.0 * li * lj / hy1;
       G[9] = P3(lj); G1[9] = P3(lj); G2[9] = P3(Lj); X[9] = 0; Y[9] = (3 * (lj * lj) - c35) / hy1;
     }
+  for (int d = 0; d < NP; ++d) {
+    double mx = 0.0;
+    for (int s2 = 0; s2 < 2; ++s2)
+      for (int a = 0; a < NG; ++a)
+        for (int b = 0; b < NG; ++b) mx = std::max(mx, std::fabs(K.phiGLL[s2][a][b][d]));
+    K.ppM[d] = mx;
+  }
   for (int g = 0; g < NG; ++g) {
     const double l = lam[g];
     const double R[NP] = {1, 1, l, c23, l, P2(l), c25, c23 * l, P2(l), P3(l)};

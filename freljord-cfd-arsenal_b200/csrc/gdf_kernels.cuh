@@ -39,6 +39,7 @@ struct Consts {
   double w[NG], lam[NG];
   double phiG[NG][NG][NP], phix[NG][NG][NP], phiy[NG][NG][NP];
   double phiGLL[2][NG][NG][NP];
+  double ppM[NP];           // max over the 50 GLL-mixed points of |phiGLL(.,.,d,.)|
   double phiGR[NG][NP], phiGL[NG][NP], phiGU[NG][NP], phiGD[NG][NP];
   double phiRU[NP], phiLU[NP], phiRD[NP], phiLD[NP];
   double mm[NP];

