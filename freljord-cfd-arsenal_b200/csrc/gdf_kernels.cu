@@ -135,8 +135,11 @@ __global__ void __launch_bounds__(128) k_face(const __grid_constant__ Consts K, 
     uL[n] = a;
     uR[n] = b;
   }
+  Side L, R;
+  make_side(K.P, uL, L);
+  make_side(K.P, uR, R);
   double Fh[NE], fL[NE], fR[NE];
-  face_flux(K.P, uL, uR, DIR, Fh, fL, fR);
+  face_flux_sides(K.P, L, R, DIR, Fh, fL, fR);
   const long long fp = DIR == 0 ? K.fxplane : K.fyplane;
   const long long o = i0 + (long long)nf * j0;
 #pragma unroll
@@ -146,14 +149,14 @@ __global__ void __launch_bounds__(128) k_face(const __grid_constant__ Consts K, 
     if (K.ez_fhat) {
       ez = -Fh[6];
     } else {
-      const double S = fmax2(fabs(uL[1] / uL[0]), fabs(uR[1] / uR[0]));
+      const double S = fmax2(fabs(L.u), fabs(R.u));
       ez = -0.5 * (fL[6] + fR[6] - S * (uR[6] - uL[6]));
     }
   } else {
     if (K.ez_fhat) {
       ez = Fh[5];
     } else {
-      const double S = fmax2(fabs(uL[2] / uL[0]), fabs(uR[2] / uR[0]));
+      const double S = fmax2(fabs(L.v), fabs(R.v));
       ez = 0.5 * (fL[5] + fR[5] - S * (uR[5] - uL[5]));
     }
   }

@@ -52,75 +52,99 @@ struct Phys {
   int eig_identity;       // eigenmatrix.f90:397-404
 };
 
-// ------------------------------------------------------------ point flux --
-// Lh.f90:88-202: conservative state -> physical flux in x (Lh FR/FL) ...
-GDF_HD void flux_x(const Phys& P, const double* U, double* F, bool drop_w_in_k) {
-  const double rho = U[0];
-  const double u = U[1] / rho, v = U[2] / rho, w = U[3] / rho;
-  const double E = U[4], B1 = U[5], B2 = U[6], B3 = U[7];
-  const double BB = sq(B1) + sq(B2) + sq(B3);
-  const double p = P.gamma1 * (E - 0.5 * rho * (sq(u) + sq(v) + sq(w)) - 0.5 * BB);
-  const double S = p + 0.5 * BB;
-  const double T = E + S;
-  const double K = drop_w_in_k ? (u * B1 + v * B2) : (u * B1 + v * B2 + w * B3);
-  F[0] = U[1];
-  F[1] = rho * sq(u) + S - sq(B1);
-  F[2] = rho * u * v - B1 * B2;
-  F[3] = rho * u * w - B1 * B3;
-  F[4] = T * u - K * B1;
+// ------------------------------------------------------------- state -----
+// A conservative state with the primitives every routine of the reference
+// derives from it (u = rhou/rho, ...; p with the com.txt gamma). Computing
+// them once and sharing them gives the same values as recomputing them in
+// each routine.
+struct Side {
+  double U[NE];
+  double rho, u, v, w, E, B1, B2, B3, BB, p;
+};
+
+GDF_HD void make_side(const Phys& P, const double* U, Side& s) {
+#pragma unroll
+  for (int n = 0; n < NE; ++n) s.U[n] = U[n];
+  s.rho = U[0];
+  s.u = U[1] / s.rho;
+  s.v = U[2] / s.rho;
+  s.w = U[3] / s.rho;
+  s.E = U[4];
+  s.B1 = U[5];
+  s.B2 = U[6];
+  s.B3 = U[7];
+  s.BB = sq(s.B1) + sq(s.B2) + sq(s.B3);
+  s.p = P.gamma1 * (s.E - 0.5 * s.rho * (sq(s.u) + sq(s.v) + sq(s.w)) - 0.5 * s.BB);
+}
+
+// Lh.f90:88-135 flux in x of a state (FR/FL arrays)
+GDF_HD void side_flux_x(const Side& s, double* F, bool drop_w_in_k) {
+  const double S = s.p + 0.5 * s.BB;
+  const double T = s.E + S;
+  const double K = drop_w_in_k ? (s.u * s.B1 + s.v * s.B2) : (s.u * s.B1 + s.v * s.B2 + s.w * s.B3);
+  F[0] = s.U[1];
+  F[1] = s.rho * sq(s.u) + S - sq(s.B1);
+  F[2] = s.rho * s.u * s.v - s.B1 * s.B2;
+  F[3] = s.rho * s.u * s.w - s.B1 * s.B3;
+  F[4] = T * s.u - K * s.B1;
   F[5] = 0.0;
-  F[6] = u * B2 - v * B1;
-  F[7] = u * B3 - w * B1;
+  F[6] = s.u * s.B2 - s.v * s.B1;
+  F[7] = s.u * s.B3 - s.w * s.B1;
 }
 
-// ... and in y (Lh FU/FD; the D side uses +u^2+v^2-w^2, Lh.f90:189).
-GDF_HD void flux_y(const Phys& P, const double* U, double* F, bool d_side) {
-  const double rho = U[0];
-  const double u = U[1] / rho, v = U[2] / rho, w = U[3] / rho;
-  const double E = U[4], B1 = U[5], B2 = U[6], B3 = U[7];
-  const double BB = sq(B1) + sq(B2) + sq(B3);
-  const double kin = d_side ? (sq(u) + sq(v) - sq(w)) : (sq(u) + sq(v) + sq(w));
-  const double p = P.gamma1 * (E - 0.5 * rho * kin - 0.5 * BB);
-  const double S = p + 0.5 * BB;
-  const double T = E + S;
-  const double K = u * B1 + v * B2 + w * B3;
-  F[0] = U[2];
-  F[1] = rho * u * v - B1 * B2;
-  F[2] = rho * sq(v) + S - sq(B2);
-  F[3] = rho * v * w - B2 * B3;
-  F[4] = T * v - K * B2;
-  F[5] = v * B1 - u * B2;
+// Lh.f90:155-202 flux in y (FU/FD); the D side takes its pressure with
+// +u^2+v^2-w^2 (Lh.f90:189)
+GDF_HD void side_flux_y(const Phys& P, const Side& s, double* F, bool d_side) {
+  const double p = d_side ? P.gamma1 * (s.E - 0.5 * s.rho * (sq(s.u) + sq(s.v) - sq(s.w)) - 0.5 * s.BB) : s.p;
+  const double S = p + 0.5 * s.BB;
+  const double T = s.E + S;
+  const double K = s.u * s.B1 + s.v * s.B2 + s.w * s.B3;
+  F[0] = s.U[2];
+  F[1] = s.rho * s.u * s.v - s.B1 * s.B2;
+  F[2] = s.rho * sq(s.v) + S - sq(s.B2);
+  F[3] = s.rho * s.v * s.w - s.B2 * s.B3;
+  F[4] = T * s.v - K * s.B2;
+  F[5] = s.v * s.B1 - s.u * s.B2;
   F[6] = 0.0;
-  F[7] = v * B3 - w * B2;
+  F[7] = s.v * s.B3 - s.w * s.B2;
 }
 
-// MHD_flux.f90:1-42 with the hard-coded gamma (note Fy(4) = rho*w*v - B3*B2).
-GDF_HD void flux_xy_hard(const Phys& P, const double* U, double* Fx, double* Fy) {
+// MHD_flux.f90 (hard-coded gamma) from a state's primitives
+GDF_HD void side_flux_hard(const Phys& P, const Side& s, double* Fx, double* Fy) {
   const double g1 = P.gflux - 1;
-  const double rho = U[0];
-  const double u = U[1] / rho, v = U[2] / rho, w = U[3] / rho;
-  const double E = U[4], B1 = U[5], B2 = U[6], B3 = U[7];
-  const double BB = sq(B1) + sq(B2) + sq(B3);
-  const double p = g1 * (E - 0.5 * rho * (sq(u) + sq(v) + sq(w)) - 0.5 * BB);
-  const double S = p + 0.5 * BB;
-  const double T = E + S;
-  const double K = u * B1 + v * B2 + w * B3;
-  Fx[0] = U[1];
-  Fx[1] = rho * sq(u) + S - sq(B1);
-  Fx[2] = rho * u * v - B1 * B2;
-  Fx[3] = rho * u * w - B1 * B3;
-  Fx[4] = T * u - K * B1;
+  const double p = g1 * (s.E - 0.5 * s.rho * (sq(s.u) + sq(s.v) + sq(s.w)) - 0.5 * s.BB);
+  const double S = p + 0.5 * s.BB;
+  const double T = s.E + S;
+  const double K = s.u * s.B1 + s.v * s.B2 + s.w * s.B3;
+  Fx[0] = s.U[1];
+  Fx[1] = s.rho * sq(s.u) + S - sq(s.B1);
+  Fx[2] = s.rho * s.u * s.v - s.B1 * s.B2;
+  Fx[3] = s.rho * s.u * s.w - s.B1 * s.B3;
+  Fx[4] = T * s.u - K * s.B1;
   Fx[5] = 0.0;
-  Fx[6] = u * B2 - v * B1;
-  Fx[7] = u * B3 - w * B1;
-  Fy[0] = U[2];
-  Fy[1] = rho * u * v - B1 * B2;
-  Fy[2] = rho * sq(v) + S - sq(B2);
-  Fy[3] = rho * w * v - B3 * B2;
-  Fy[4] = T * v - K * B2;
-  Fy[5] = v * B1 - u * B2;
+  Fx[6] = s.u * s.B2 - s.v * s.B1;
+  Fx[7] = s.u * s.B3 - s.w * s.B1;
+  Fy[0] = s.U[2];
+  Fy[1] = s.rho * s.u * s.v - s.B1 * s.B2;
+  Fy[2] = s.rho * sq(s.v) + S - sq(s.B2);
+  Fy[3] = s.rho * s.w * s.v - s.B3 * s.B2;
+  Fy[4] = T * s.v - K * s.B2;
+  Fy[5] = s.v * s.B1 - s.u * s.B2;
   Fy[6] = 0.0;
-  Fy[7] = v * B3 - w * B2;
+  Fy[7] = s.v * s.B3 - s.w * s.B2;
+}
+
+// eigenvalueMm.f90 from a state's primitives (normal x: dir 0, y: dir 1)
+GDF_HD void side_speeds(const Phys& P, const Side& s, int dir, double& amax, double& amin) {
+  const double Bn = dir == 0 ? s.B1 : s.B2;
+  const double un = dir == 0 ? s.u : s.v;
+  const double c = sqrt(fabs(P.gamma * s.p / s.rho));
+  const double c2 = sq(c);
+  const double br = s.BB / s.rho;
+  const double X = c2 + br;
+  const double cf = sqrt(fabs(0.5 * (c2 + br + sqrt(sq(X) - 4 * c2 * sq(Bn) / s.rho))));
+  amax = un + cf;
+  amin = un - cf;
 }
 
 // -------------------------------------------------------- wave speeds ------
@@ -142,61 +166,31 @@ GDF_HD void fast_speeds(const Phys& P, const double* U, int dir, double& amax, d
 }
 
 // ------------------------------------------------------ 1-D Riemann --------
-// State on each side of a face and its physical flux; "R" is the state on
-// the +normal side, as in the reference's UR1/FR1 (Lh.f90:216-219).
-struct Face1 {
-  double UR[NE], UL[NE], FR[NE], FL[NE];
-  double SR, SL;
-};
-
-// LF_Flux.f90:5
-GDF_HD void lf_flux(const Face1& f, double* Fh) {
-  const double a = fmax2(fabs(f.SR), fabs(f.SL));
-#pragma unroll
-  for (int n = 0; n < NE; ++n) Fh[n] = 0.5 * (f.FR[n] + f.FL[n] - a * (f.UR[n] - f.UL[n]));
-}
-
-// HLL_Flux.f90:5-11
-GDF_HD void hll_flux(const Face1& f, double* Fh) {
-  const double SR = f.SR, SL = f.SL;
-  if (SR < 0) {
-#pragma unroll
-    for (int n = 0; n < NE; ++n) Fh[n] = f.FR[n];
-  } else if (SL > 0) {
-#pragma unroll
-    for (int n = 0; n < NE; ++n) Fh[n] = f.FL[n];
-  } else {
-    const double den = SR - SL, sls = SL * SR;
-#pragma unroll
-    for (int n = 0; n < NE; ++n) Fh[n] = (SR * f.FL[n] - SL * f.FR[n] + sls * (f.UR[n] - f.UL[n])) / den;
-  }
-}
-
 // HLLC_Flux.f90:9-106 and HLLD_Flux.f90:14-189 share the first stage.
 // dir 0 = normal x (reference direction 1), 1 = normal y (direction 2).
 // Fh gets the flux, Ust the star state (Ustar of the reference).
 template <bool HLLD>
-GDF_HD void hllcd_flux(const Phys& P, Face1& f, int dir, double* Fh, double* Ust) {
-  const double SR = f.SR, SL = f.SL;
+GDF_HD void hllcd_flux(const Phys& P, const Side& R, const Side& L, const double* FR, const double* FL, double SR,
+                       double SL, int dir, double* Fh, double* Ust) {
   if (SR < 0) {
 #pragma unroll
-    for (int n = 0; n < NE; ++n) { Fh[n] = f.FR[n]; Ust[n] = f.UR[n]; }
+    for (int n = 0; n < NE; ++n) { Fh[n] = FR[n]; Ust[n] = R.U[n]; }
     return;
   }
   if (SL > 0) {
 #pragma unroll
-    for (int n = 0; n < NE; ++n) { Fh[n] = f.FL[n]; Ust[n] = f.UL[n]; }
+    for (int n = 0; n < NE; ++n) { Fh[n] = FL[n]; Ust[n] = L.U[n]; }
     return;
   }
-  const double* UR1 = f.UR;
-  const double* UL1 = f.UL;
+  const double* UR1 = R.U;
+  const double* UL1 = L.U;
   double Us[NE];
 #pragma unroll
-  for (int n = 0; n < NE; ++n) Us[n] = (SR * UR1[n] - SL * UL1[n] + f.FL[n] - f.FR[n]) / (SR - SL);
-  const double rhoR = UR1[0], u1R = UR1[1] / rhoR, u2R = UR1[2] / rhoR, u3R = UR1[3] / rhoR, ER = UR1[4];
-  const double B1R = UR1[5], B2R = UR1[6], B3R = UR1[7];
-  const double rhoL = UL1[0], u1L = UL1[1] / rhoL, u2L = UL1[2] / rhoL, u3L = UL1[3] / rhoL, EL = UL1[4];
-  const double B1L = UL1[5], B2L = UL1[6], B3L = UL1[7];
+  for (int n = 0; n < NE; ++n) Us[n] = (SR * UR1[n] - SL * UL1[n] + FL[n] - FR[n]) / (SR - SL);
+  const double rhoR = R.rho, u1R = R.u, u2R = R.v, u3R = R.w, ER = R.E;
+  const double B1R = R.B1, B2R = R.B2, B3R = R.B3;
+  const double rhoL = L.rho, u1L = L.u, u2L = L.v, u3L = L.w, EL = L.E;
+  const double B1L = L.B1, B2L = L.B2, B3L = L.B3;
   const double Sstar = (dir == 0 ? Us[1] : Us[2]) / Us[0];
   const double uRbot = dir == 0 ? u1R : u2R, uLbot = dir == 0 ? u1L : u2L;
   const double BRbot = dir == 0 ? B1R : B2R, BLbot = dir == 0 ? B1L : B2L;
@@ -262,10 +256,10 @@ GDF_HD void hllcd_flux(const Phys& P, Face1& f, int dir, double* Fh, double* Ust
   if (HLLD && (fabs(Bsb) > P.hlld_eps) && (SRs - SLs > P.hlld_eps)) {
     if (SLs > 0) {
 #pragma unroll
-      for (int n = 0; n < NE; ++n) { Fh[n] = f.FL[n] + SL * (ULs[n] - UL1[n]); Ust[n] = ULs[n]; }
+      for (int n = 0; n < NE; ++n) { Fh[n] = FL[n] + SL * (ULs[n] - UL1[n]); Ust[n] = ULs[n]; }
     } else if (SRs < 0) {
 #pragma unroll
-      for (int n = 0; n < NE; ++n) { Fh[n] = f.FR[n] + SR * (URs[n] - UR1[n]); Ust[n] = URs[n]; }
+      for (int n = 0; n < NE; ++n) { Fh[n] = FR[n] + SR * (URs[n] - UR1[n]); Ust[n] = URs[n]; }
     } else {
       // second stage (HLLD_Flux.f90:134-176)
       const double sL = sqrt(fabs(rhoLs)), sR = sqrt(fabs(rhoRs));
@@ -284,7 +278,7 @@ GDF_HD void hllcd_flux(const Phys& P, Face1& f, int dir, double* Fh, double* Ust
         const double Uss[NE] = {rhoLs, rhoLs * u1ss, rhoLs * u2ss, rhoLs * u3ss, ELss, B1ss, B2ss, B3ss};
 #pragma unroll
         for (int n = 0; n < NE; ++n) {
-          const double FLm = f.FL[n] + SL * (ULs[n] - UL1[n]);
+          const double FLm = FL[n] + SL * (ULs[n] - UL1[n]);
           Fh[n] = FLm + SLs * (Uss[n] - ULs[n]);
           Ust[n] = Uss[n];
         }
@@ -294,7 +288,7 @@ GDF_HD void hllcd_flux(const Phys& P, Face1& f, int dir, double* Fh, double* Ust
         const double Uss[NE] = {rhoRs, rhoRs * u1ss, rhoRs * u2ss, rhoRs * u3ss, ERss, B1ss, B2ss, B3ss};
 #pragma unroll
         for (int n = 0; n < NE; ++n) {
-          const double FRm = f.FR[n] + SR * (URs[n] - UR1[n]);
+          const double FRm = FR[n] + SR * (URs[n] - UR1[n]);
           Fh[n] = FRm + SRs * (Uss[n] - URs[n]);
           Ust[n] = Uss[n];
         }
@@ -303,43 +297,62 @@ GDF_HD void hllcd_flux(const Phys& P, Face1& f, int dir, double* Fh, double* Ust
   } else {
     if (Sstar > 0) {
 #pragma unroll
-      for (int n = 0; n < NE; ++n) { Fh[n] = f.FL[n] + SL * (ULs[n] - UL1[n]); Ust[n] = ULs[n]; }
+      for (int n = 0; n < NE; ++n) { Fh[n] = FL[n] + SL * (ULs[n] - UL1[n]); Ust[n] = ULs[n]; }
     } else {
 #pragma unroll
-      for (int n = 0; n < NE; ++n) { Fh[n] = f.FR[n] + SR * (URs[n] - UR1[n]); Ust[n] = URs[n]; }
+      for (int n = 0; n < NE; ++n) { Fh[n] = FR[n] + SR * (URs[n] - UR1[n]); Ust[n] = URs[n]; }
     }
   }
 }
 
 // Riemann solve at one face point. uL = state on the -normal side (the
 // reference's UL1), uR = +normal side (UR1); dir 0 = x, 1 = y. Writes the
-// numerical flux Fh and returns the fluxes of both sides in fL / fR.
-GDF_HD void face_flux(const Phys& P, const double* uL, const double* uR, int dir, double* Fh, double* fL,
-                      double* fR) {
-  Face1 f;
-#pragma unroll
-  for (int n = 0; n < NE; ++n) { f.UL[n] = uL[n]; f.UR[n] = uR[n]; }
+// numerical flux Fh and returns the fluxes of both sides in fL / fR and the
+// normal velocities of both sides in unL / unR (used by the face Ez).
+GDF_HD void face_flux_sides(const Phys& P, const Side& L, const Side& R, int dir, double* Fh, double* fL,
+                            double* fR) {
   if (dir == 0) {
-    flux_x(P, uL, f.FL, false);
-    flux_x(P, uR, f.FR, !P.kml_w);
+    side_flux_x(L, fL, false);
+    side_flux_x(R, fR, !P.kml_w);
   } else {
-    flux_y(P, uL, f.FL, false);
-    flux_y(P, uR, f.FR, true);
+    side_flux_y(P, L, fL, false);
+    side_flux_y(P, R, fR, true);
   }
   double a1, a2, b1, b2;
-  fast_speeds(P, uL, dir, a1, a2);   // SRmax/SRmin of the reference (from UR(i) = left side)
-  fast_speeds(P, uR, dir, b1, b2);   // SLmax/SLmin (from UL(i+1) = right side)
-  f.SR = fmax2(a1, b1);
-  f.SL = fmin2(a2, b2);
+  side_speeds(P, L, dir, a1, a2);   // SRmax/SRmin of the reference (from UR(i) = left side)
+  side_speeds(P, R, dir, b1, b2);   // SLmax/SLmin (from UL(i+1) = right side)
+  const double SR = fmax2(a1, b1);
+  const double SL = fmin2(a2, b2);
   double Ust[NE];
-  switch (P.flux) {
-    case 1: lf_flux(f, Fh); break;
-    case 2: hll_flux(f, Fh); break;
-    case 3: hllcd_flux<false>(P, f, dir, Fh, Ust); break;
-    default: hllcd_flux<true>(P, f, dir, Fh, Ust); break;
-  }
+  if (P.flux == 1) {
+    const double a = fmax2(fabs(SR), fabs(SL));
 #pragma unroll
-  for (int n = 0; n < NE; ++n) { fL[n] = f.FL[n]; fR[n] = f.FR[n]; }
+    for (int n = 0; n < NE; ++n) Fh[n] = 0.5 * (fR[n] + fL[n] - a * (R.U[n] - L.U[n]));
+  } else if (P.flux == 2) {
+    if (SR < 0) {
+#pragma unroll
+      for (int n = 0; n < NE; ++n) Fh[n] = fR[n];
+    } else if (SL > 0) {
+#pragma unroll
+      for (int n = 0; n < NE; ++n) Fh[n] = fL[n];
+    } else {
+      const double den = SR - SL, sls = SL * SR;
+#pragma unroll
+      for (int n = 0; n < NE; ++n) Fh[n] = (SR * fL[n] - SL * fR[n] + sls * (R.U[n] - L.U[n])) / den;
+    }
+  } else if (P.flux == 3) {
+    hllcd_flux<false>(P, R, L, fR, fL, SR, SL, dir, Fh, Ust);
+  } else {
+    hllcd_flux<true>(P, R, L, fR, fL, SR, SL, dir, Fh, Ust);
+  }
+}
+
+GDF_HD void face_flux(const Phys& P, const double* uL, const double* uR, int dir, double* Fh, double* fL,
+                      double* fR) {
+  Side L, R;
+  make_side(P, uL, L);
+  make_side(P, uR, R);
+  face_flux_sides(P, L, R, dir, Fh, fL, fR);
 }
 
 // ------------------------------------------------------ 2-D vertex Ez -----
@@ -373,24 +386,29 @@ GDF_HD double vertex_ez(const Phys& P, const double* URU, const double* ULU, con
     return 0.25 * (EzRU + EzLU + EzRD + EzLD) - 0.25 * ay * (0.5 * (URU[5] + ULU[5]) - 0.5 * (URD[5] + ULD[5])) +
            0.25 * ax * (0.5 * (URU[6] + URD[6]) - 0.5 * (ULU[6] + ULD[6]));
   }
+  Side sRU, sLU, sRD, sLD;
+  make_side(P, URU, sRU);
+  make_side(P, ULU, sLU);
+  make_side(P, URD, sRD);
+  make_side(P, ULD, sLD);
   double axRU, bxRU, ayRU, byRU, axLU, bxLU, ayLU, byLU, axRD, bxRD, ayRD, byRD, axLD, bxLD, ayLD, byLD;
-  fast_speeds(P, URU, 0, axRU, bxRU);
-  fast_speeds(P, URU, 1, ayRU, byRU);
-  fast_speeds(P, ULU, 0, axLU, bxLU);
-  fast_speeds(P, ULU, 1, ayLU, byLU);
-  fast_speeds(P, URD, 0, axRD, bxRD);
-  fast_speeds(P, URD, 1, ayRD, byRD);
-  fast_speeds(P, ULD, 0, axLD, bxLD);
-  fast_speeds(P, ULD, 1, ayLD, byLD);
+  side_speeds(P, sRU, 0, axRU, bxRU);
+  side_speeds(P, sRU, 1, ayRU, byRU);
+  side_speeds(P, sLU, 0, axLU, bxLU);
+  side_speeds(P, sLU, 1, ayLU, byLU);
+  side_speeds(P, sRD, 0, axRD, bxRD);
+  side_speeds(P, sRD, 1, ayRD, byRD);
+  side_speeds(P, sLD, 0, axLD, bxLD);
+  side_speeds(P, sLD, 1, ayLD, byLD);
   const double SR = fmax2(fmax2(fmax2(axRU, axLU), axRD), axLD);
   const double SL = fmin2(fmin2(fmin2(bxRU, bxLU), bxRD), bxLD);
   const double SU = fmax2(fmax2(fmax2(ayRU, ayLU), ayRD), ayLD);
   const double SD = fmin2(fmin2(fmin2(byRU, byLU), byRD), byLD);
   double FxRU[NE], FyRU[NE], FxLU[NE], FyLU[NE], FxRD[NE], FyRD[NE], FxLD[NE], FyLD[NE];
-  flux_xy_hard(P, URU, FxRU, FyRU);
-  flux_xy_hard(P, ULU, FxLU, FyLU);
-  flux_xy_hard(P, URD, FxRD, FyRD);
-  flux_xy_hard(P, ULD, FxLD, FyLD);
+  side_flux_hard(P, sRU, FxRU, FyRU);
+  side_flux_hard(P, sLU, FxLU, FyLU);
+  side_flux_hard(P, sRD, FxRD, FyRD);
+  side_flux_hard(P, sLD, FxLD, FyLD);
   double EzRs, EzLs, EzUs, EzDs;
   if (P.flux == 2) {
     double BxUs, BxDs, ByRs, ByLs, fU7, fD7;
@@ -419,21 +437,17 @@ GDF_HD double vertex_ez(const Phys& P, const double* URU, const double* ULU, con
   }
   // HLLC / HLLD vertex solvers: four 1-D solves, plain average for Ez**
   double Fh[NE], Us[NE];
-  Face1 f;
-  auto solve = [&](const double* Ur, const double* Ul, const double* Fr, const double* Fl, double sr, double sl,
-                   int dir) {
-#pragma unroll
-    for (int n = 0; n < NE; ++n) { f.UR[n] = Ur[n]; f.UL[n] = Ul[n]; f.FR[n] = Fr[n]; f.FL[n] = Fl[n]; }
-    f.SR = sr; f.SL = sl;
-    if (P.flux == 3) hllcd_flux<false>(P, f, dir, Fh, Us); else hllcd_flux<true>(P, f, dir, Fh, Us);
+  auto solve = [&](const Side& r, const Side& l, const double* Fr, const double* Fl, double sr, double sl, int dir) {
+    if (P.flux == 3) hllcd_flux<false>(P, r, l, Fr, Fl, sr, sl, dir, Fh, Us);
+    else hllcd_flux<true>(P, r, l, Fr, Fl, sr, sl, dir, Fh, Us);
   };
-  solve(URU, ULU, FxRU, FxLU, SR, SL, 0);
+  solve(sRU, sLU, FxRU, FxLU, SR, SL, 0);
   EzUs = -Fh[6];
-  solve(URD, ULD, FxRD, FxLD, SR, SL, 0);
+  solve(sRD, sLD, FxRD, FxLD, SR, SL, 0);
   EzDs = -Fh[6];
-  solve(URU, URD, FyRU, FyRD, SU, SD, 1);
+  solve(sRU, sRD, FyRU, FyRD, SU, SD, 1);
   EzRs = Fh[5];
-  solve(ULU, ULD, FyLU, FyLD, SU, SD, 1);
+  solve(sLU, sLD, FyLU, FyLD, SU, SD, 1);
   EzLs = Fh[5];
   if (SL > 0) return EzLs;
   if (SR < 0) return EzRs;
