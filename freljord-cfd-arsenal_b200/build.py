@@ -26,8 +26,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 HOST_CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 
 KERNEL_SRC = os.path.join(CSRC, "gdf_kernels.cu")
+MLP_SRC = os.path.join(CSRC, "gdf_mlp.cu")
 HOST_SRC = os.path.join(CSRC, "gdf_host.cpp")
-HEADERS = [os.path.join(CSRC, f) for f in ("gdf_physics.cuh", "gdf_kernels.cuh")] + [
+HEADERS = [os.path.join(CSRC, f) for f in ("gdf_physics.cuh", "gdf_kernels.cuh", "gdf_mlp.cuh")] + [
     os.path.join(REPO, "include", "gdf.h")]
 
 
@@ -63,16 +64,19 @@ def build(verbose: bool = False) -> dict:
     out = {}
     for name, flags in (("libgdf_b200.so", ["--fmad=false", "-DGDF_EXACT=1"]),
                         ("libgdf_b200_fma.so", ["--fmad=true"])):
-        obj = os.path.join(BUILD, name.replace(".so", ".o"))
+        objs = []
+        for src in (KERNEL_SRC, MLP_SRC):
+            obj = os.path.join(BUILD, name.replace(".so", "") + "_" + os.path.basename(src).replace(".cu", ".o"))
+            if _stale(obj, [src] + HEADERS):
+                cmd = [nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17", *flags,
+                       "-Xcompiler", "-fPIC,-ffp-contract=off", "-c", src, "-o", obj]
+                if verbose:
+                    cmd.insert(1, "-Xptxas=-v")
+                _run(cmd)
+            objs.append(obj)
         so = os.path.join(LIB, name)
-        if _stale(obj, [KERNEL_SRC] + HEADERS):
-            cmd = [nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17", *flags,
-                   "-Xcompiler", "-fPIC,-ffp-contract=off", "-c", KERNEL_SRC, "-o", obj]
-            if verbose:
-                cmd.insert(1, "-Xptxas=-v")
-            _run(cmd)
-        if _stale(so, [obj, host_o]):
-            _run([nvcc, *ARCH, "-shared", "-o", so, obj, host_o])
+        if _stale(so, objs + [host_o]):
+            _run([nvcc, *ARCH, "-shared", "-o", so, *objs, host_o])
         out[name] = so
     return out
 

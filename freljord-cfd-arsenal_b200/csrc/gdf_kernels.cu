@@ -32,6 +32,7 @@
 
 #include "../../include/gdf.h"
 #include "gdf_kernels.cuh"
+#include "gdf_mlp.cuh"
 
 #ifndef GDF_EXACT
 #define GDF_EXACT 0
@@ -422,6 +423,113 @@ __global__ void __launch_bounds__(128) k_bface(const __grid_constant__ Consts K,
   }
 }
 
+// ------------------------------------------- learned-indicator features ---
+// Per cell (ghosts included) the first six P2 modes of rho (copied), of the
+// pressure and of |B|^2 (L2 projections with a 3x3 Gauss rule, in FP32):
+// 18 floats per cell, QM[(q*6 + d) * plane + cell], q = rho, p, |B|^2.
+// These feed the troubled-cell network; the FP64 solver state is untouched.
+constexpr int QMODES = 18;
+
+__device__ __forceinline__ float basis10(int d, float x, float y) {
+  switch (d) {
+    case 0: return 1.f;
+    case 1: return x;
+    case 2: return y;
+    case 3: return x * x - (1.f / 3.f);
+    case 4: return x * y;
+    case 5: return y * y - (1.f / 3.f);
+    case 6: return x * x * x - 0.6f * x;
+    case 7: return (x * x - (1.f / 3.f)) * y;
+    case 8: return x * (y * y - (1.f / 3.f));
+    default: return y * y * y - 0.6f * y;
+  }
+}
+
+__global__ void k_qmodes(const __grid_constant__ Consts K, const double* __restrict__ S, float* __restrict__ QM) {
+  const long long c = gtid();
+  if (c >= K.plane) return;
+  const float gx[3] = {-0.7745966692414834f, 0.f, 0.7745966692414834f};
+  const float gw[3] = {5.f / 9.f, 8.f / 9.f, 5.f / 9.f};
+  const float mmf[6] = {1.f, 1.f / 3.f, 1.f / 3.f, 4.f / 45.f, 1.f / 9.f, 4.f / 45.f};
+  float m[NE][NP];
+#pragma unroll
+  for (int n = 0; n < NE; ++n)
+#pragma unroll
+    for (int d = 0; d < NP; ++d) m[n][d] = live_mode(n, d) ? (float)S[c + K.plane * (d + 10 * n)] : 0.f;
+  float pm[6], bm[6];
+#pragma unroll
+  for (int d = 0; d < 6; ++d) { pm[d] = 0.f; bm[d] = 0.f; }
+  const float g1 = (float)K.P.gamma1;
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      float v[NE];
+#pragma unroll
+      for (int n = 0; n < NE; ++n) {
+        float x = 0.f;
+#pragma unroll
+        for (int d = 0; d < NP; ++d)
+          if (live_mode(n, d)) x += m[n][d] * basis10(d, gx[a], gx[b]);
+        v[n] = x;
+      }
+      const float rho = v[0];
+      const float b2 = v[5] * v[5] + v[6] * v[6] + v[7] * v[7];
+      const float kin = (v[1] * v[1] + v[2] * v[2] + v[3] * v[3]) / rho;
+      const float pr = g1 * (v[4] - 0.5f * kin - 0.5f * b2);
+      const float wq = gw[a] * gw[b] * 0.25f;
+#pragma unroll
+      for (int d = 0; d < 6; ++d) {
+        const float ph = basis10(d, gx[a], gx[b]);
+        pm[d] += wq * ph * pr;
+        bm[d] += wq * ph * b2;
+      }
+    }
+#pragma unroll
+  for (int d = 0; d < 6; ++d) {
+    QM[(long long)d * K.plane + c] = m[0][d];
+    QM[(long long)(6 + d) * K.plane + c] = pm[d] / mmf[d];
+    QM[(long long)(12 + d) * K.plane + c] = bm[d] / mmf[d];
+  }
+}
+
+// The 90 inputs of interior cell (i, j): for the cell and its neighbours
+// (i+1,j), (i-1,j), (i,j+1), (i,j-1), the 6 modes of rho, p, |B|^2, each
+// quantity scaled by the largest |mean| over the five cells, with the
+// cell's own mean subtracted from the means; clamped to [-8, 8].
+constexpr int NFEAT = 90;
+__device__ __forceinline__ void gather_features(const Consts& K, const float* __restrict__ QM, long long c,
+                                                float* out /* 90 */) {
+  const long long nb[5] = {c, c + 1, c - 1, c + K.nx2, c - K.nx2};
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    float sc = 0.f;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) sc = fmaxf(sc, fabsf(QM[(long long)(q * 6) * K.plane + nb[k]]));
+    sc = sc + 1e-30f;
+    const float inv = 1.f / sc;
+    const float mean_c = QM[(long long)(q * 6) * K.plane + c];
+#pragma unroll
+    for (int k = 0; k < 5; ++k)
+#pragma unroll
+      for (int d = 0; d < 6; ++d) {
+        float v = QM[(long long)(q * 6 + d) * K.plane + nb[k]];
+        if (d == 0) v -= mean_c;
+        out[(k * 3 + q) * 6 + d] = fminf(8.f, fmaxf(-8.f, v * inv));
+      }
+  }
+}
+
+__global__ void k_features(const __grid_constant__ Consts K, const float* __restrict__ QM, float* __restrict__ X) {
+  const long long item = gtid();
+  if (item >= (long long)K.nx * K.ny) return;
+  const int i = (int)(item % K.nx) + 1, j = (int)(item / K.nx) + 1;
+  float f[NFEAT];
+  gather_features(K, QM, i + (long long)K.nx2 * j, f);
+#pragma unroll
+  for (int k = 0; k < NFEAT; ++k) X[item * NFEAT + k] = f[k];
+}
+
 // ------------------------------------------------------------ limiter ----
 // TVB_Limiter_P2.f90:16-121 (characteristic TVB, Jacobi over cells), with
 // KXRCF_Detector.f90 as gate, pp_Limiter.f90, and div_free_Balsara.f90:13-79
@@ -646,18 +754,47 @@ __device__ void pp_cell(const Consts& K, double (*m)[NP]) {
     for (int d = 1; d < NP; ++d) m[n][d] = eta * m[n][d];
 }
 
+template <bool LEARNED>
 __global__ void __launch_bounds__(LIM_BS) k_limit(const __grid_constant__ Consts K, const double* __restrict__ S,
                                                   double* __restrict__ D, const double* __restrict__ BX,
                                                   const double* __restrict__ BY, int32_t* __restrict__ flags,
                                                   int32_t* __restrict__ trouble, int stage, int divfree,
-                                                  const Scal* __restrict__ gate_sc, Scal* __restrict__ sc) {
+                                                  const Scal* __restrict__ gate_sc, Scal* __restrict__ sc,
+                                                  const MlpDev* __restrict__ net, const float* __restrict__ QM,
+                                                  float t_lo, float t_hi) {
+  extern __shared__ __align__(16) unsigned char lsm[];
   if (gate_sc && !gate_sc->active) return;
   const long long item = gtid();
-  if (item >= (long long)K.nx * K.ny) return;
-  const int i = (int)(item % K.nx) + 1;
-  const int j = (int)(item / K.nx) + 1;
+  const bool valid = item < (long long)K.nx * K.ny;
+  const int i = valid ? (int)(item % K.nx) + 1 : 1;
+  const int j = valid ? (int)(item / K.nx) + 1 : 1;
   const long long c = i + (long long)K.nx2 * j;
   const long long pl = K.plane;
+  float p_net = 0.f;
+  if (LEARNED) {
+    // the learned indicator for the block's 64 cells on the tensor cores
+    __nv_bfloat16* Xs = reinterpret_cast<__nv_bfloat16*>(lsm);
+    __nv_bfloat16* W1t = Xs + LIM_BS * MLP_LDX;
+    __nv_bfloat16* W2t = W1t + MLP_H * MLP_LDX;
+    __nv_bfloat16* H1 = W2t + MLP_H * MLP_LDH;
+    float* zz = reinterpret_cast<float*>(H1 + LIM_BS * MLP_LDH);
+    const int tid = threadIdx.x;
+    for (int k = tid; k < MLP_H * MLP_INP; k += LIM_BS) W1t[(k / MLP_INP) * MLP_LDX + k % MLP_INP] = net->W1t[k];
+    for (int k = tid; k < MLP_H * MLP_H; k += LIM_BS) W2t[(k / MLP_H) * MLP_LDH + k % MLP_H] = net->W2t[k];
+    float f[NFEAT];
+    if (valid) {
+      gather_features(K, QM, c, f);
+    } else {
+#pragma unroll
+      for (int k = 0; k < NFEAT; ++k) f[k] = 0.f;
+    }
+#pragma unroll
+    for (int k = 0; k < MLP_INP; ++k) Xs[tid * MLP_LDX + k] = __float2bfloat16_rn(k < NFEAT ? f[k] : 0.f);
+    __syncthreads();
+    mlp_infer_tiles(Xs, W1t, W2t, net->b1, net->b2, net->w3, net->b3, H1, zz, LIM_BS);
+    p_net = 1.f / (1.f + expf(-zz[tid]));
+  }
+  if (!valid) return;
   double m[NE][NP];
 #pragma unroll
   for (int n = 0; n < NE; ++n)
@@ -670,6 +807,12 @@ __global__ void __launch_bounds__(LIM_BS) k_limit(const __grid_constant__ Consts
     // a set sticky flag stays set whatever the detector finds
     gate = prev ? true : kxrcf_flag(K, S, c, m, prev);
     trouble[item] = gate ? 1 : 0;
+    if (gate) word |= (1 << 24);
+  } else if (LEARNED) {
+    // confident network answers decide; KXRCF decides in the uncertain band
+    if (p_net >= t_hi) gate = true;
+    else if (p_net >= t_lo) gate = kxrcf_flag(K, S, c, m, false);
+    else gate = false;
     if (gate) word |= (1 << 24);
   }
   if (gate) {
@@ -1073,6 +1216,9 @@ struct GdfHandle {
   double *BX = nullptr, *BX0 = nullptr, *BXI = nullptr, *BY = nullptr, *BY0 = nullptr, *BYI = nullptr;
   double *Fxh = nullptr, *Fyh = nullptr, *EzRL = nullptr, *EzUD = nullptr, *EzV = nullptr;
   double *part = nullptr;
+  float* QM = nullptr;       // learned-indicator feature modes (18 per cell)
+  MlpDev* net = nullptr;     // learned-indicator network (device copy)
+  float t_lo = 0.5f, t_hi = 0.5f;
   int32_t *flags = nullptr, *trouble = nullptr;
   Scal* sc = nullptr;
   Scal* sc_host = nullptr;  // pinned mirror
@@ -1222,7 +1368,8 @@ static int check_config(const GdfConfig* c) {
   if (c->flux_type < 1 || c->flux_type > 4) return fail(GDF_ERR_ARG, "flux_type must be 1..4");
   if (!(c->gamma > 1.0) || !(c->gamma_flux > 1.0)) return fail(GDF_ERR_ARG, "gamma must be > 1");
   if (!(c->cfl > 0.0)) return fail(GDF_ERR_ARG, "cfl must be > 0");
-  if (c->detector != GDF_DETECT_ALL && c->detector != GDF_DETECT_KXRCF) return fail(GDF_ERR_ARG, "unknown detector");
+  if (c->detector != GDF_DETECT_ALL && c->detector != GDF_DETECT_KXRCF && c->detector != GDF_DETECT_LEARNED)
+    return fail(GDF_ERR_ARG, "unknown detector");
   return GDF_OK;
 }
 
@@ -1260,9 +1407,22 @@ static int launch_limit(GdfHandle* h, const double* S, double* D, int stage, con
   const Consts& K = h->K;
   const long long ncell = (long long)K.nx * K.ny;
   const int fused_divfree = K.faceb ? 0 : 1;
+  size_t smem = 0;
+  if (K.detector == GDF_DETECT_LEARNED) {
+    if (!h->net || !h->QM) return fail(GDF_ERR_STATE, "detector GDF_DETECT_LEARNED needs gdf_set_indicator first");
+    int rq = run_kernel(h, GDF_K_LIMIT, [&] { k_qmodes<<<nblk(K.plane, 128), 128, 0, h->st>>>(K, S, h->QM); });
+    if (rq) return rq;
+    smem = (size_t)(LIM_BS + MLP_H) * MLP_LDX * 2 + (size_t)(MLP_H + LIM_BS) * MLP_LDH * 2 + LIM_BS * sizeof(float);
+  }
   int rc0 = run_kernel(h, GDF_K_LIMIT, [&] {
-    k_limit<<<nblk(ncell, LIM_BS), LIM_BS, 0, h->st>>>(K, S, D, h->BX, h->BY, h->flags, h->trouble, stage,
-                                                       fused_divfree, sc_gate, h->sc);
+    if (K.detector == GDF_DETECT_LEARNED)
+      k_limit<true><<<nblk(ncell, LIM_BS), LIM_BS, smem, h->st>>>(K, S, D, h->BX, h->BY, h->flags, h->trouble, stage,
+                                                                  fused_divfree, sc_gate, h->sc, h->net, h->QM,
+                                                                  h->t_lo, h->t_hi);
+    else
+      k_limit<false><<<nblk(ncell, LIM_BS), LIM_BS, 0, h->st>>>(K, S, D, h->BX, h->BY, h->flags, h->trouble, stage,
+                                                                fused_divfree, sc_gate, h->sc, nullptr, nullptr,
+                                                                0.f, 0.f);
   });
   if (rc0) return rc0;
   if (K.faceb) {
@@ -1442,6 +1602,8 @@ int gdf_destroy(GdfHandle* h) {
                     h->Fxh, h->Fyh, h->EzRL, h->EzUD, h->EzV, h->part};
   for (double* p : bufs)
     if (p) cudaFree(p);
+  if (h->QM) cudaFree(h->QM);
+  if (h->net) cudaFree(h->net);
   if (h->flags) cudaFree(h->flags);
   if (h->trouble) cudaFree(h->trouble);
   if (h->sc) cudaFree(h->sc);
@@ -1614,6 +1776,43 @@ int gdf_lh_noalloc(const GdfConfig* cfg, const double* d_uh, double* d_du, void*
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(GDF_ERR_CUDA, std::string("gdf_lh_noalloc launch: ") + cudaGetErrorString(e));
   return GDF_OK;
+}
+
+extern "C" const void* gdf_mlp_device_params(GdfMlp* m);
+
+int gdf_set_indicator(GdfHandle* h, GdfMlp* m, float t_lo, float t_hi) {
+  if (!h || !m) return fail(GDF_ERR_ARG, "null argument");
+  if (!(t_lo <= t_hi)) return fail(GDF_ERR_ARG, "t_lo must not exceed t_hi");
+  if (!h->net) CK(cudaMalloc((void**)&h->net, sizeof(MlpDev)));
+  if (!h->QM) CK(cudaMalloc((void**)&h->QM, (size_t)QMODES * h->K.plane * sizeof(float)));
+  CK(cudaMemcpy(h->net, gdf_mlp_device_params(m), sizeof(MlpDev), cudaMemcpyDeviceToDevice));
+  h->t_lo = t_lo;
+  h->t_hi = t_hi;
+  if (h->graph) {   // the captured step holds the old kernel arguments
+    cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+  }
+  return GDF_OK;
+}
+
+int gdf_features(GdfHandle* h, const double* uh, float* X) {
+  if (!h || !uh || !X) return fail(GDF_ERR_ARG, "null argument");
+  int rc = check_dead_slots(h->cfg, uh);
+  if (rc) return rc;
+  const long long ncell = (long long)h->cfg.nx * h->cfg.ny;
+  if (!h->QM) CK(cudaMalloc((void**)&h->QM, (size_t)QMODES * h->K.plane * sizeof(float)));
+  float* dX = nullptr;
+  CK(cudaMallocAsync((void**)&dX, (size_t)ncell * NFEAT * sizeof(float), h->st));
+  CK(cudaMemcpyAsync(h->UT, uh, uh_bytes(h->cfg), cudaMemcpyHostToDevice, h->st));
+  rc = run_kernel(h, GDF_K_LIMIT, [&] { k_qmodes<<<nblk(h->K.plane, 128), 128, 0, h->st>>>(h->K, h->UT, h->QM); });
+  if (!rc) rc = run_kernel(h, GDF_K_LIMIT, [&] { k_features<<<nblk(ncell, 128), 128, 0, h->st>>>(h->K, h->QM, dX); });
+  if (!rc) {
+    cudaError_t e = cudaMemcpyAsync(X, dX, (size_t)ncell * NFEAT * sizeof(float), cudaMemcpyDeviceToHost, h->st);
+    if (e != cudaSuccess) rc = fail(GDF_ERR_CUDA, cudaGetErrorString(e));
+  }
+  cudaFreeAsync(dX, h->st);
+  CK(cudaStreamSynchronize(h->st));
+  return rc;
 }
 
 int gdf_set_device(int32_t device) {

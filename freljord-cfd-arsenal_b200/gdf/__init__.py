@@ -28,6 +28,10 @@ from ._abi import (BC_OUTFLOW, BC_PERIODIC, DETECT_ALL, DETECT_KXRCF, FLUX_HLL, 
                    PROB_ROTOR, PROB_VORTEX, GdfConfig, bx_shape, by_shape, dptr, iptr, new_state,
                    problem_config, reference_config, uh_shape)
 
+DETECT_LEARNED = 2
+MLP_NPARAM = 10049
+NFEAT = 90
+
 KERNEL_NAMES = ["set_bc", "face_x", "face_y", "vertex", "cell", "bface", "limit", "dt", "diag"]
 KERNEL_KINDS = len(KERNEL_NAMES)
 
@@ -83,6 +87,17 @@ def load(exact: bool = True):
     L.gdf_advance_timed.argtypes = [vp, C.c_double, i32, dp, ip, dp]
     L.gdf_set_device.argtypes = [i32]
     L.gdf_lh_noalloc.argtypes = [cfgp, vp, vp, vp]
+    fp = C.POINTER(C.c_float)
+    L.gdf_features.argtypes = [vp, dp, fp]
+    L.gdf_mlp_create.argtypes = [i32, C.POINTER(vp)]
+    L.gdf_mlp_destroy.argtypes = [vp]
+    L.gdf_mlp_set_params.argtypes = [vp, fp]
+    L.gdf_mlp_get_params.argtypes = [vp, fp]
+    L.gdf_mlp_grad.argtypes = [vp, fp, fp, C.c_int64, C.c_float, fp, fp]
+    L.gdf_mlp_train.argtypes = [vp, fp, fp, C.c_int64, i32, i32, C.c_float, C.c_float, i32, fp]
+    L.gdf_mlp_predict.argtypes = [vp, fp, C.c_int64, fp]
+    L.gdf_mlp_last_error.restype = C.c_char_p
+    L.gdf_set_indicator.argtypes = [vp, vp, C.c_float, C.c_float]
     _libs[path] = L
     return L
 
@@ -156,6 +171,15 @@ class Solver:
         uh, bx, by = new_state(self.nx, self.ny)
         _check(self.L, self.L.gdf_download(self.h, dptr(uh), dptr(bx), dptr(by)))
         return uh, bx, by
+
+    def features(self, uh):
+        """gdf_features: the indicator's 90 inputs per interior cell."""
+        X = np.zeros((self.nx * self.ny, NFEAT), np.float32)
+        _check(self.L, self.L.gdf_features(self.h, dptr(uh), X.ctypes.data_as(C.POINTER(C.c_float))))
+        return X
+
+    def set_indicator(self, mlp: "Mlp", t_lo: float = 0.5, t_hi: float = 0.5) -> None:
+        _check(self.L, self.L.gdf_set_indicator(self.h, mlp.h, t_lo, t_hi))
 
     def download_into(self, uh, bx, by) -> None:
         """gdf_download into caller arrays (e.g. pinned host buffers)."""
@@ -240,3 +264,69 @@ class Solver:
         _check(self.L, self.L.gdf_profile(self.h, steps, dptr(ms), n.ctypes.data_as(C.POINTER(C.c_int64)),
                                           KERNEL_KINDS))
         return {KERNEL_NAMES[k]: (ms[k], int(n[k])) for k in range(KERNEL_KINDS)}
+
+
+def _fptr(a: np.ndarray):
+    assert a.dtype == np.float32 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class Mlp:
+    """The learned troubled-cell indicator (90-64-64-1), trained and run by
+    the library's tensor-core kernels."""
+
+    def __init__(self, seed: int = 0, exact: bool = True):
+        self.L = load(exact)
+        h = C.c_void_p()
+        rc = self.L.gdf_mlp_create(seed, C.byref(h))
+        if rc:
+            raise GdfError(rc, self.L.gdf_mlp_last_error().decode())
+        self.h = h
+
+    def _ck(self, rc):
+        if rc:
+            raise GdfError(rc, self.L.gdf_mlp_last_error().decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.gdf_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def params(self) -> np.ndarray:
+        p = np.zeros(MLP_NPARAM, np.float32)
+        self._ck(self.L.gdf_mlp_get_params(self.h, _fptr(p)))
+        return p
+
+    def set_params(self, p) -> None:
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == MLP_NPARAM
+        self._ck(self.L.gdf_mlp_set_params(self.h, _fptr(p)))
+
+    def grad(self, X, y, pos_weight: float = 1.0):
+        X = np.ascontiguousarray(X, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        g = np.zeros(MLP_NPARAM, np.float32)
+        loss = np.zeros(1, np.float32)
+        self._ck(self.L.gdf_mlp_grad(self.h, _fptr(X), _fptr(y), len(y), pos_weight, _fptr(g), _fptr(loss)))
+        return g, float(loss[0])
+
+    def train(self, X, y, epochs: int = 10, batch: int = 1024, lr: float = 1e-3, pos_weight: float = 1.0,
+              seed: int = 0):
+        X = np.ascontiguousarray(X, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        losses = np.zeros(epochs, np.float32)
+        self._ck(self.L.gdf_mlp_train(self.h, _fptr(X), _fptr(y), len(y), epochs, batch, lr, pos_weight, seed,
+                                      _fptr(losses)))
+        return losses
+
+    def predict(self, X):
+        X = np.ascontiguousarray(X, np.float32)
+        p = np.zeros(len(X), np.float32)
+        self._ck(self.L.gdf_mlp_predict(self.h, _fptr(X), len(X), _fptr(p)))
+        return p

@@ -55,7 +55,9 @@ enum { GDF_BC_PERIODIC = 1, GDF_BC_OUTFLOW = 2 };
  * (TVB_Limiter_P2.f90:12,22). */
 enum {
   GDF_DETECT_ALL = 0,    /* reference as shipped: every cell is limited    */
-  GDF_DETECT_KXRCF = 1   /* KXRCF_Detector.f90 gates the limiter           */
+  GDF_DETECT_KXRCF = 1,  /* KXRCF_Detector.f90 gates the limiter           */
+  GDF_DETECT_LEARNED = 2 /* the learned indicator (gdf_set_indicator) gates
+                            the limiter; KXRCF decides where it is unsure  */
 };
 
 /* Initial-data problems (init_data.f90:3-19 include list; sizes and
@@ -171,6 +173,39 @@ int gdf_lh(GdfHandle *h, const double *uh, double *du);
 int gdf_lhez(GdfHandle *h, const double *uh, double *dez1, double *dez2);
 int gdf_limit(GdfHandle *h, double *uh, double *bx, double *by, int32_t *flags);
 int gdf_dt(GdfHandle *h, const double *uh, double *dt);
+
+/* Inputs of the learned troubled-cell indicator for every interior cell of
+ * uh (a state as gdf_limit takes it, ghosts set): X[(i-1) + Nx*(j-1)][90],
+ * the 6 P2 modes of rho, pressure and |B|^2 of the cell and its four
+ * neighbours, scaled per cell. No counterpart in the reference (whose only
+ * detector is KXRCF_Detector.f90). */
+int gdf_features(GdfHandle *h, const double *uh, float *X);
+
+/* ---- learned troubled-cell indicator (no counterpart in the reference) ---
+ * A 90-64-64-1 network (GELU, GELU, sigmoid) on the gdf_features inputs,
+ * trained by the library's own kernels (BF16 tensor-core products, FP32
+ * accumulation, Adam on FP32 master weights). Parameters are packed FP32:
+ * W1[90][64], b1[64], W2[64][64], b2[64], w3[64], b3 (10049 values). */
+#define GDF_MLP_NPARAM 10049
+typedef struct GdfMlp GdfMlp;
+int gdf_mlp_create(int32_t seed, GdfMlp **out);   /* Glorot init from seed */
+int gdf_mlp_destroy(GdfMlp *m);
+int gdf_mlp_set_params(GdfMlp *m, const float *params);   /* resets Adam */
+int gdf_mlp_get_params(GdfMlp *m, float *params);
+/* Gradient of the mean weighted binary cross-entropy (positives weighted
+ * pos_weight) over all n samples X[n][90], y[n] in {0,1}. */
+int gdf_mlp_grad(GdfMlp *m, const float *X, const float *y, int64_t n, float pos_weight,
+                 float *grad, float *loss);
+/* Adam (lr, betas 0.9/0.999) over shuffled minibatches; epoch_loss (may be
+ * NULL) receives the mean loss of each epoch. */
+int gdf_mlp_train(GdfMlp *m, const float *X, const float *y, int64_t n, int32_t epochs,
+                  int32_t batch, float lr, float pos_weight, int32_t seed, float *epoch_loss);
+int gdf_mlp_predict(GdfMlp *m, const float *X, int64_t n, float *p);
+const char *gdf_mlp_last_error(void);
+/* Use the network m (copied) as the troubled-cell detector of h when its
+ * config has detector GDF_DETECT_LEARNED: the limiter runs where p >= t_hi,
+ * and where t_lo <= p < t_hi if KXRCF flags the cell. */
+int gdf_set_indicator(GdfHandle *h, GdfMlp *m, float t_lo, float t_hi);
 
 /* Lh (as gdf_lh) on caller-owned DEVICE buffers, allocating no device
  * memory: d_uh and d_du are device pointers with the uh extents of the
