@@ -163,6 +163,99 @@ def cpu_baseline(gdf, steps: int):
             "seconds": el}
 
 
+def learned_blast(gdf, steps: int):
+    """Plain (KXRCF) vs learned-indicator throughput on the MHD blast.
+
+    Whole runs at 512^2 (t = 0.01, every step timed) give the throughput of
+    both methods over the blast's evolution and the L1 density difference
+    learned vs plain; at 2048^2, `steps` steps from the start of the run
+    (after 3 warm-up steps) are timed for both."""
+    from gdf.indicator import WEIGHTS, load_net, run
+    import numpy as np
+    net, lo, hi = load_net(WEIGHTS)
+    out = {"weights": os.path.relpath(WEIGHTS, REPO), "t_lo": lo, "t_hi": hi}
+    u_p, st_p, ms_p, g_p = run(512, 0, None, params="default")
+    u_l, st_l, ms_l, g_l = run(512, 0, net, lo, hi, params="default")
+    rho_p, rho_l = u_p[0, 0, 1:-1, 1:-1], u_l[0, 0, 1:-1, 1:-1]
+    out["blast512_full_run"] = {
+        "plain": {"value": 512 * 512 / (ms_p / 1e3), "ms_per_step": ms_p, "steps": st_p,
+                  "gated_cells_per_step": g_p},
+        "learned": {"value": 512 * 512 / (ms_l / 1e3), "ms_per_step": ms_l, "steps": st_l,
+                    "gated_cells_per_step": g_l},
+        "speedup": ms_p * st_p / (ms_l * st_l),
+        "l1_rho_learned_vs_plain": float(np.abs(rho_l - rho_p).mean() / np.abs(rho_p).mean())}
+    n = 2048
+    res = {}
+    for name, det in (("plain", gdf.DETECT_KXRCF), ("learned", gdf.DETECT_LEARNED)):
+        cfg, tend = gdf.problem_config(gdf.PROB_BLAST, n, n)
+        cfg.detector = det
+        uh, bx, by = gdf.init_data(cfg, gdf.PROB_BLAST)
+        s = gdf.Solver(cfg)
+        if det == gdf.DETECT_LEARNED:
+            s.set_indicator(net, lo, hi)
+        s.upload(uh, bx, by)
+        s.prepare()
+        s.advance_timed(tend, 3)
+        _, k, ms = s.advance_timed(tend, steps)
+        res[name] = {"value": n * n * k / (ms / 1e3), "ms_per_step": ms / k, "steps": k}
+        s.close()
+    res["speedup"] = res["plain"]["ms_per_step"] / res["learned"]["ms_per_step"]
+    out["blast2048_first_steps"] = res
+    return out
+
+
+def ensemble_bench(gdf, steps: int):
+    """The 64-instance ensemble (Orszag-Tang / rotor / blast, sides 64..512,
+    HLLD): the plain GPU path (one handle per instance, KXRCF, graph
+    replays, instances one after another), the batched plain method, and
+    the batched learned-indicator method (autotuned tile shape)."""
+    from gdf.indicator import WEIGHTS, load_net
+    net, lo, hi = load_net(WEIGHTS)
+    items = gdf.ensemble_configs(64, 0)
+    cells = [c.nx * c.ny for c, _, _, _ in items]
+    states = [gdf.init_data(c, p, prm) for c, p, prm, _ in items]
+    out = {"instances": len(items), "cells": int(sum(cells)), "sides": sorted({c.nx for c, _, _, _ in items})}
+    # plain, one instance at a time
+    cu, tot_ms = 0, 0.0
+    for (c, p, prm, tend), st in zip(items, states):
+        cp = c.copy()
+        cp.detector = gdf.DETECT_KXRCF
+        s = gdf.Solver(cp)
+        s.upload(*st)
+        s.prepare()
+        s.advance_timed(tend, 3)
+        _, k, ms = s.advance_timed(tend, steps)
+        cu += k * cp.nx * cp.ny
+        tot_ms += ms
+        s.close()
+    out["plain_sequential"] = {"value": cu / (tot_ms / 1e3), "ms_per_step": tot_ms / steps}
+    for name, learned in (("batched_plain", False), ("batched_learned", True)):
+        cfgs = []
+        for c, _, _, _ in items:
+            cc = c.copy()
+            cc.detector = gdf.DETECT_LEARNED if learned else gdf.DETECT_KXRCF
+            cfgs.append(cc)
+        e = gdf.Ensemble(cfgs)
+        if learned:
+            e.set_indicator(net, lo, hi)
+        for i, st in enumerate(states):
+            e.upload(i, *st)
+        e.prepare()
+        for i, (_, _, _, tend) in enumerate(items):
+            e.set_time(i, 0.0, tend)
+        e.advance(2)
+        tune_ms = e.tune(1)
+        e.advance(1)
+        l0 = e.kernel_launches()
+        cu, act, ms = e.advance(steps)
+        out[name] = {"value": cu / (ms / 1e3), "ms_per_step": ms / steps, "tiles": e.tiles(),
+                     "launches_per_step": (e.kernel_launches() - l0) / steps,
+                     "tuner_best_ms": float(min(x for x in tune_ms if x > 0))}
+        e.close()
+    out["speedup_batched_learned_vs_plain"] = out["batched_learned"]["value"] / out["plain_sequential"]["value"]
+    return out
+
+
 def run_reference(args):
     world, rank, _ = dist_env()
     if rank != 0:
@@ -296,6 +389,11 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(gdf, args.cpu_steps)
 
+    learned = ens = None
+    if not args.no_extra:
+        learned = learned_blast(gdf, args.steps)
+        ens = ensemble_bench(gdf, args.steps)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -315,6 +413,8 @@ def run_ours(args):
                     "d2h_bytes_per_step": int(io_bytes), "steps": e2e_steps},
             "cpu_baseline": cpu,
             "fma_build": fma,
+            "learned_indicator": learned,
+            "ensemble": ens,
             "build": "libgdf_b200.so (no FMA contraction: value-exact with the reference arithmetic)",
             "clocks": clocks,
             "steps_taken": taken,
@@ -336,6 +436,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-fma", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the learned-indicator and ensemble runs")
     ap.add_argument("--quick", action="store_true", help="timed steps only (for profiler captures)")
     ap.add_argument("--fma", action="store_true", help="with --quick: run the FMA build")
     args = ap.parse_args()

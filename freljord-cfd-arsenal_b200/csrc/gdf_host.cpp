@@ -186,6 +186,10 @@ int gdf_problem_config(int32_t problem, int32_t nx, int32_t ny, GdfConfig* out, 
       out->pp_limiter = 1;
       out->detector = GDF_DETECT_KXRCF;
       out->kxrcf_ck = 1.0;
+      // the face-B minmod of the DF variants (TVB_Limiter_P2.f90:186-187
+      // applied): with HLLD and the raw face B the strong blasts of this
+      // family lose positivity within tens of steps
+      out->faceb_limiter = 1;
       te = 0.01;
       break;
     case GDF_PROB_CLOUD_SHOCK:

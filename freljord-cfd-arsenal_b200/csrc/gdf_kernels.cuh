@@ -16,6 +16,9 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <string>
+
+#include "../../include/gdf.h"
 
 #include "gdf_physics.cuh"
 
@@ -55,5 +58,12 @@ struct Scal {
   long long steps;    // steps taken since upload
   long long troubled; // cells flagged by the last step
 };
+
+// Host helpers shared by the single-problem handle and the ensemble
+// (gdf_kernels.cu): the constants of a configuration, and the checks of a
+// configuration and of an uploaded state (0 or a GDF_ERR_* code with msg).
+void consts_for(const GdfConfig& c, Consts& K);
+int config_error(const GdfConfig* c, std::string& msg);
+int dead_slot_error(const GdfConfig& c, const double* uh, std::string& msg);
 
 }  // namespace gdf

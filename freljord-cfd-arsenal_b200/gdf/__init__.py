@@ -98,6 +98,21 @@ def load(exact: bool = True):
     L.gdf_mlp_predict.argtypes = [vp, fp, C.c_int64, fp]
     L.gdf_mlp_last_error.restype = C.c_char_p
     L.gdf_set_indicator.argtypes = [vp, vp, C.c_float, C.c_float]
+    L.gdf_ens_create.argtypes = [cfgp, i32, C.POINTER(vp)]
+    L.gdf_ens_destroy.argtypes = [vp]
+    L.gdf_ens_upload.argtypes = [vp, i32, dp, dp, dp]
+    L.gdf_ens_download.argtypes = [vp, i32, dp, dp, dp]
+    L.gdf_ens_set_indicator.argtypes = [vp, vp, C.c_float, C.c_float]
+    L.gdf_ens_set_time.argtypes = [vp, i32, C.c_double, C.c_double]
+    L.gdf_ens_get_time.argtypes = [vp, i32, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int64)]
+    L.gdf_ens_prepare.argtypes = [vp]
+    L.gdf_ens_advance.argtypes = [vp, i32, C.POINTER(C.c_int64), C.POINTER(i32), C.POINTER(C.c_double)]
+    L.gdf_ens_set_tiles.argtypes = [vp, i32, i32, i32]
+    L.gdf_ens_get_tiles.argtypes = [vp] + [C.POINTER(i32)] * 5
+    L.gdf_ens_tune.argtypes = [vp, i32, C.POINTER(C.c_float)]
+    L.gdf_ens_kernel_launches.argtypes = [vp]
+    L.gdf_ens_kernel_launches.restype = C.c_int64
+    L.gdf_ens_last_error.restype = C.c_char_p
     _libs[path] = L
     return L
 
@@ -330,3 +345,103 @@ class Mlp:
         p = np.zeros(len(X), np.float32)
         self._ck(self.L.gdf_mlp_predict(self.h, _fptr(X), len(X), _fptr(p)))
         return p
+
+
+class Ensemble:
+    """Independent problems of different sizes advanced together (the
+    gdf_ens_* functions): one persistent kernel per RK stage, per-instance
+    dt and end time."""
+
+    def __init__(self, cfgs, exact: bool = True):
+        self.L = load(exact)
+        self.cfgs = [c.copy() for c in cfgs]
+        arr = (GdfConfig * len(self.cfgs))(*self.cfgs)
+        h = C.c_void_p()
+        self._ck(self.L.gdf_ens_create(arr, len(self.cfgs), C.byref(h)))
+        self.h = h
+        self.n = len(self.cfgs)
+
+    def _ck(self, rc):
+        if rc:
+            raise GdfError(rc, self.L.gdf_ens_last_error().decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.gdf_ens_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, i: int, uh, bx, by) -> None:
+        self._ck(self.L.gdf_ens_upload(self.h, i, dptr(uh), dptr(bx), dptr(by)))
+
+    def download(self, i: int):
+        c = self.cfgs[i]
+        uh, bx, by = new_state(c.nx, c.ny)
+        self._ck(self.L.gdf_ens_download(self.h, i, dptr(uh), dptr(bx), dptr(by)))
+        return uh, bx, by
+
+    def set_indicator(self, mlp: "Mlp", t_lo: float = 0.5, t_hi: float = 0.5) -> None:
+        self._ck(self.L.gdf_ens_set_indicator(self.h, mlp.h, t_lo, t_hi))
+
+    def set_time(self, i: int, t: float, tend: float) -> None:
+        """t and tend of instance i (i = -1: every instance)."""
+        self._ck(self.L.gdf_ens_set_time(self.h, i, t, tend))
+
+    def time(self, i: int):
+        t, dt, n = C.c_double(), C.c_double(), C.c_int64()
+        self._ck(self.L.gdf_ens_get_time(self.h, i, C.byref(t), C.byref(dt), C.byref(n)))
+        return t.value, dt.value, n.value
+
+    def prepare(self) -> None:
+        self._ck(self.L.gdf_ens_prepare(self.h))
+
+    def advance(self, steps: int):
+        """(cell updates, instances still running, device ms) of `steps`
+        ensemble steps."""
+        cu, na, ms = C.c_int64(), C.c_int32(), C.c_double()
+        self._ck(self.L.gdf_ens_advance(self.h, steps, C.byref(cu), C.byref(na), C.byref(ms)))
+        return cu.value, na.value, ms.value
+
+    def set_tiles(self, ctas_per_sm: int = 0, face_per_thread: int = 1, cell_per_thread: int = 1) -> None:
+        self._ck(self.L.gdf_ens_set_tiles(self.h, ctas_per_sm, face_per_thread, cell_per_thread))
+
+    def tiles(self) -> dict:
+        v = [C.c_int32() for _ in range(5)]
+        self._ck(self.L.gdf_ens_get_tiles(self.h, *[C.byref(x) for x in v]))
+        return dict(zip(["ctas_per_sm", "face_per_thread", "cell_per_thread", "grid", "graph"], [x.value for x in v]))
+
+    def tune(self, steps: int = 2):
+        ms = np.zeros(36, np.float32)
+        self._ck(self.L.gdf_ens_tune(self.h, steps, _fptr(ms)))
+        return ms
+
+    def kernel_launches(self) -> int:
+        return self.L.gdf_ens_kernel_launches(self.h)
+
+
+def ensemble_configs(n: int = 64, seed: int = 0, detector: int = DETECT_LEARNED):
+    """The ensemble workload: instance s takes, from a generator seeded by
+    (seed, s), a problem in {Orszag-Tang, rotor, blast} and a square grid side
+    in {64, 96, ..., 512}; all HLLD, the given detector (KXRCF fallback when
+    learned). Returns [(config, problem, init params or None, tend)]."""
+    out = []
+    for s in range(n):
+        rng = np.random.default_rng([seed, s])
+        prob = [PROB_ORSZAG_TANG, PROB_ROTOR, PROB_BLAST][int(rng.integers(3))]
+        side = 64 + 32 * int(rng.integers(15))
+        cfg, tend = problem_config(prob, side, side)
+        cfg.flux_type = FLUX_HLLD
+        cfg.detector = detector
+        if detector != DETECT_ALL:
+            cfg.kxrcf_ck = 1.0
+        params = None
+        if prob == PROB_BLAST:
+            from .indicator import blast_params
+            params = blast_params(10_000 + 97 * seed + s)
+        out.append((cfg, prob, params, tend))
+    return out

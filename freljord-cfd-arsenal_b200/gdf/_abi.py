@@ -121,6 +121,7 @@ def problem_config(problem: int, nx: int, ny: int) -> tuple[GdfConfig, float]:
         c.detector = DETECT_KXRCF
         c.kxrcf_ck = 1.0
         c.tvb_m = 10.0
+        c.faceb_limiter = 1                # DF-variant face-B minmod (robustness)
         tend = 0.01
     elif problem == PROB_CLOUD_SHOCK:     # init6.txt (the reference default)
         c.xa, c.xb, c.ya, c.yb = 0.0, 2.0, 0.0, 1.0

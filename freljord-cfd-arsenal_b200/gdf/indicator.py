@@ -1,0 +1,304 @@
+"""Training data, training, thresholds and evaluation of the learned
+troubled-cell indicator (no counterpart in the reference, which uses
+KXRCF_Detector.f90 alone).
+
+Data. Seeded MHD blasts (centre uniform in [-0.2, 0.2]^2, radius 0.1,
+rho = 1, outer pressure 0.1, inner/outer pressure ratio log-uniform in
+[1e2, 1e4], |B| uniform in [0, 100/sqrt(4 pi)] at a uniform angle, gamma
+1.4, HLLD, KXRCF + TVB + positivity limiter) run on the device with the
+plain solver. At sampled steps the stage-1 pre-limit state u + dt L(u) is
+formed (Lh, LhEz and calculate_dt through the C ABI), and each interior cell
+gets its 90 inputs (gdf_features) and the label
+
+    y = KXRCF flags the cell (per stage, not sticky)
+        AND the characteristic TVB limiter changes it (detector ALL),
+
+i.e. the cells where the reference's trigger leads to a modified solution.
+Smooth cells (y = 0) far outnumber the rest and are subsampled.
+
+Gate. With thresholds t_lo <= t_hi the limiter runs where p >= t_hi, not
+where p < t_lo, and KXRCF decides in between; (0, 0) is the all-cells
+limiter and (0, > 1) is per-stage KXRCF exactly. The positivity limiter and
+the divergence-free reconstruction always run unchanged in FP64.
+
+Run as a module:
+    python -m gdf.indicator train --out weights.npy   (data, training, thresholds)
+    python -m gdf.indicator eval --weights weights.npy --n 512 --seeds 1001 1002
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import time
+
+import numpy as np
+
+from . import (DETECT_ALL, DETECT_KXRCF, DETECT_LEARNED, NFEAT, PROB_BLAST, Mlp, Solver, init_data,
+               problem_config)
+
+WEIGHTS = os.path.join(os.path.dirname(__file__), "data", "indicator_blast256.npz")
+STAGE_CHANGE = 0xFFFFFF       # per-stage change masks of the flag word
+GATE_BIT = 1 << 24            # stage-1 gate bit of the flag word
+
+
+def blast_params(seed: int) -> np.ndarray:
+    """init_data parameters (cx, cy, r0, p_in, p_out, rho, Bx, By) of the
+    seeded blast."""
+    rng = np.random.default_rng(seed)
+    cx, cy = rng.uniform(-0.2, 0.2, 2)
+    ratio = math.exp(rng.uniform(math.log(1e2), math.log(1e4)))
+    bmag = rng.uniform(0.0, 100.0 / math.sqrt(4 * math.pi))
+    ang = rng.uniform(0.0, 2 * math.pi)
+    p_out = 0.1
+    return np.array([cx, cy, 0.1, p_out * ratio, p_out, 1.0, bmag * math.cos(ang), bmag * math.sin(ang)])
+
+
+def blast_setup(n: int, seed: int, detector: int = DETECT_KXRCF, sticky: int = 1, exact: bool = True,
+                params=None):
+    """Config and initial state of the seeded blast on n x n cells (params
+    "default": the benchmark blast, p = 1000 inside r = 0.1 at the centre,
+    Bx = By = 100/sqrt(8 pi))."""
+    cfg, tend = problem_config(PROB_BLAST, n, n)
+    cfg.detector = detector
+    cfg.kxrcf_sticky = sticky
+    prm = None if params == "default" else (blast_params(seed) if params is None else params)
+    uh, bx, by = init_data(cfg, PROB_BLAST, prm, exact=exact)
+    return cfg, tend, uh, bx, by
+
+
+class Labeller:
+    """Stage-1 pre-limit states, their inputs and labels, on one grid size."""
+
+    def __init__(self, cfg, exact: bool = True):
+        a = cfg.copy()
+        a.detector = DETECT_ALL
+        k = cfg.copy()
+        k.detector = DETECT_KXRCF
+        k.kxrcf_sticky = 0
+        self.s_all = Solver(a, exact)
+        self.s_kx = Solver(k, exact)
+
+    def prelimit(self, uh, bx, by):
+        """u + dt L(u) for a state whose ghost cells are set (RK3.f90:60-100)."""
+        s = self.s_all
+        du = s.lh(uh)
+        d1, d2 = s.lhez(uh)
+        dt = s.dt(uh)
+        return uh + dt * du, bx + dt * d1, by + dt * d2
+
+    def sample(self, uh, bx, by):
+        """(X [ncell, 90] float32, y [ncell] bool, kxrcf [ncell] bool,
+        change [ncell] bool) of the stage-1 pre-limit state of uh."""
+        ui, bi, ci = self.prelimit(uh, bx, by)
+        X = self.s_all.features(ui)
+        fa = self.s_all.limit(ui.copy(), bi.copy(), ci.copy()).ravel()
+        fk = self.s_kx.limit(ui.copy(), bi.copy(), ci.copy()).ravel()
+        change = (fa & STAGE_CHANGE) != 0
+        kx = (fk & GATE_BIT) != 0
+        return X, change & kx, kx, change
+
+
+def collect(n: int, seeds, samples_per_run: int = 6, neg_keep: float = 0.15, exact: bool = True, log=None):
+    """Labelled cells from seeded blasts of n x n cells: every positive and a
+    `neg_keep` share of the negatives (seeded)."""
+    Xs, ys = [], []
+    lab = None
+    for seed in seeds:
+        cfg, tend, uh, bx, by = blast_setup(n, seed, exact=exact)
+        if lab is None:
+            lab = Labeller(cfg, exact)
+        s = Solver(cfg, exact)
+        s.upload(uh, bx, by)
+        s.prepare()
+        rng = np.random.default_rng(10_000 + seed)
+        for k in range(samples_per_run):
+            t_k = tend * (k + 0.5) / samples_per_run
+            s.advance(t_k, 10**7)
+            u, b, c = s.download()
+            X, y, _, _ = lab.sample(u, b, c)
+            keep = y | (rng.random(y.size) < neg_keep)
+            Xs.append(X[keep])
+            ys.append(y[keep].astype(np.float32))
+        s.close()
+        if log:
+            log(f"seed {seed}: {sum(len(v) for v in ys)} samples so far, positives {sum(v.sum() for v in ys):.0f}")
+    return np.concatenate(Xs), np.concatenate(ys)
+
+
+def choose_thresholds(p, y, miss: float = 0.002, fp: float = 0.002):
+    """t_lo: the largest threshold missing at most `miss` of the positives
+    below it; t_hi: the smallest threshold passing at most `fp` of the
+    negatives above it (t_hi >= t_lo)."""
+    y = y > 0.5
+    pp = np.sort(p[y])
+    pn = np.sort(p[~y])
+    t_lo = float(pp[int(math.floor(miss * len(pp)))]) if len(pp) else 1.0
+    t_hi = float(pn[min(len(pn) - 1, int(math.ceil((1 - fp) * len(pn))))]) if len(pn) else 0.0
+    t_hi = max(t_hi, t_lo)
+    return t_lo, t_hi
+
+
+def train(X, y, seed: int = 0, epochs: int = 12, batch: int = 2048, lr: float = 2e-3, exact: bool = True,
+          val_frac: float = 0.1, log=None):
+    """Train on the device (the library's forward, backward and Adam
+    kernels); returns (net, t_lo, t_hi, report)."""
+    rng = np.random.default_rng(seed)
+    order = rng.permutation(len(y))
+    nval = int(val_frac * len(y))
+    iv, it = order[:nval], order[nval:]
+    pos = float(y[it].sum())
+    pos_weight = float((len(it) - pos) / max(pos, 1.0))
+    net = Mlp(seed, exact)
+    t0 = time.time()
+    losses = net.train(X[it], y[it], epochs=epochs, batch=batch, lr=lr, pos_weight=pos_weight, seed=seed)
+    t_train = time.time() - t0
+    pv = net.predict(X[iv])
+    t_lo, t_hi = choose_thresholds(pv, y[iv])
+    yv = y[iv] > 0.5
+    band = (pv >= t_lo) & (pv < t_hi)
+    rep = {"samples": int(len(y)), "positives": int(y.sum()), "pos_weight": pos_weight,
+           "epoch_loss": [float(v) for v in losses], "train_s": t_train,
+           "val_accuracy_at_0.5": float(np.mean((pv >= 0.5) == yv)),
+           "t_lo": t_lo, "t_hi": t_hi, "val_band_share": float(band.mean()),
+           "val_miss_below_t_lo": float(np.mean(pv[yv] < t_lo)) if yv.any() else 0.0,
+           "val_fp_above_t_hi": float(np.mean(pv[~yv] >= t_hi)) if (~yv).any() else 0.0}
+    if log:
+        log(json.dumps(rep))
+    return net, t_lo, t_hi, rep
+
+
+def save(path: str, net: Mlp, t_lo: float, t_hi: float, report: dict) -> None:
+    os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+    np.savez(path, params=net.params(), t_lo=np.float32(t_lo), t_hi=np.float32(t_hi),
+             report=json.dumps(report))
+
+
+def load_net(path: str = WEIGHTS, exact: bool = True):
+    """(net, t_lo, t_hi) from a saved indicator."""
+    z = np.load(path)
+    net = Mlp(0, exact)
+    net.set_params(z["params"])
+    return net, float(z["t_lo"]), float(z["t_hi"])
+
+
+def run(n: int, seed: int, net=None, t_lo=0.5, t_hi=0.5, exact: bool = True, tend=None, max_steps=10**7,
+        params=None, detector=None, sticky: int = 1):
+    """Seeded blast to tend with the plain method (net None: KXRCF, sticky,
+    as the reference; or `detector`) or the learned gate; returns (uh,
+    steps, ms per step, mean cells flagged in a step)."""
+    det = (DETECT_KXRCF if detector is None else detector) if net is None else DETECT_LEARNED
+    cfg, te, uh, bx, by = blast_setup(n, seed, det, sticky=sticky, exact=exact, params=params)
+    s = Solver(cfg, exact)
+    if net is not None:
+        s.set_indicator(net, t_lo, t_hi)
+    s.upload(uh, bx, by)
+    s.prepare()
+    t_end = te if tend is None else tend
+    steps, ms = 0, 0.0
+    gated, chunks = 0, 0
+    while s.t < t_end and steps < max_steps:
+        _, k, dms = s.advance_timed(t_end, min(200, max_steps - steps))
+        if k == 0:
+            break
+        steps += k
+        ms += dms
+        gated += s.diagnostics()[3]
+        chunks += 1
+    u, _, _ = s.download()
+    s.close()
+    return u, steps, ms / max(steps, 1), gated / max(chunks, 1)
+
+
+def restrict_means(u_fine, n):
+    """Cell means of an (2n)^2 state averaged onto the n^2 grid."""
+    r = u_fine[:, 0, 1:-1, 1:-1]
+    return 0.25 * (r[:, 0::2, 0::2] + r[:, 1::2, 0::2] + r[:, 0::2, 1::2] + r[:, 1::2, 1::2])
+
+
+def evaluate(net, t_lo, t_hi, n: int, seeds, ref_factor: int = 2, samples: int = 4, exact: bool = True,
+             log=None):
+    """Held-out evaluation: L1 density error of the plain and learned runs
+    against a plain run on a grid ref_factor times finer, the L1 difference
+    learned vs plain, and the gate's miss / false-positive rates against the
+    labels along the plain trajectory."""
+    out = []
+    for seed in seeds:
+        u_p, st_p, ms_p, g_p = run(n, seed, None, exact=exact)
+        u_l, st_l, ms_l, g_l = run(n, seed, net, t_lo, t_hi, exact=exact)
+        rho_p, rho_l = u_p[0, 0, 1:-1, 1:-1], u_l[0, 0, 1:-1, 1:-1]
+        h2 = 1.0 / (n * n)
+        rec = {"seed": seed, "n": n, "steps_plain": st_p, "steps_learned": st_l,
+               "ms_per_step_plain": ms_p, "ms_per_step_learned": ms_l,
+               "gated_per_step_plain": g_p, "gated_per_step_learned": g_l,
+               "l1_rho_learned_vs_plain": float(np.abs(rho_l - rho_p).sum() * h2),
+               "l1_rho_plain": float(np.abs(rho_p).sum() * h2)}
+        if ref_factor:
+            u_f, _, _, _ = run(n * ref_factor, seed, None, exact=exact)
+            rho_f = restrict_means(u_f, n)[0] if ref_factor == 2 else None
+            rec["l1_err_plain"] = float(np.abs(rho_p - rho_f).sum() * h2)
+            rec["l1_err_learned"] = float(np.abs(rho_l - rho_f).sum() * h2)
+            rec["l1_err_ratio"] = rec["l1_err_learned"] / rec["l1_err_plain"]
+        # gate quality along the plain trajectory
+        cfg, tend, uh, bx, by = blast_setup(n, seed, exact=exact)
+        lab = Labeller(cfg, exact)
+        s = Solver(cfg, exact)
+        s.upload(uh, bx, by)
+        s.prepare()
+        tp = fn = fp = tn = band = 0
+        for k in range(samples):
+            s.advance(tend * (k + 0.5) / samples, 10**7)
+            X, y, kx, _ = lab.sample(*s.download())
+            p = net.predict(X)
+            gate = (p >= t_hi) | ((p >= t_lo) & kx)
+            tp += int(np.sum(gate & y)); fn += int(np.sum(~gate & y))
+            fp += int(np.sum(gate & ~y)); tn += int(np.sum(~gate & ~y))
+            band += int(np.sum((p >= t_lo) & (p < t_hi)))
+        s.close()
+        rec.update({"miss_rate": fn / max(tp + fn, 1), "false_positive_rate": fp / max(fp + tn, 1),
+                    "band_share": band / max(tp + fn + fp + tn, 1), "positives": tp + fn,
+                    "cells_sampled": tp + fn + fp + tn})
+        if log:
+            log(json.dumps(rec))
+        out.append(rec)
+    return out
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(prog="python -m gdf.indicator")
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    t = sub.add_parser("train")
+    t.add_argument("--n", type=int, default=256)
+    t.add_argument("--seeds", type=int, default=24)
+    t.add_argument("--samples-per-run", type=int, default=6)
+    t.add_argument("--neg-keep", type=float, default=0.15)
+    t.add_argument("--epochs", type=int, default=12)
+    t.add_argument("--out", default=WEIGHTS)
+    e = sub.add_parser("eval")
+    e.add_argument("--weights", default=WEIGHTS)
+    e.add_argument("--n", type=int, default=512)
+    e.add_argument("--seeds", type=int, nargs="+", default=[1001, 1002])
+    e.add_argument("--ref-factor", type=int, default=2)
+    e.add_argument("--out", default=None)
+    a = ap.parse_args(argv)
+    log = lambda m: print(m, flush=True)  # noqa: E731
+    if a.cmd == "train":
+        t0 = time.time()
+        X, y = collect(a.n, range(a.seeds), a.samples_per_run, a.neg_keep, log=log)
+        log(f"collected {len(y)} cells ({int(y.sum())} positive) in {time.time() - t0:.1f} s")
+        net, t_lo, t_hi, rep = train(X, y, epochs=a.epochs, log=log)
+        rep.update({"grid": a.n, "train_seeds": a.seeds, "samples_per_run": a.samples_per_run,
+                    "neg_keep": a.neg_keep})
+        save(a.out, net, t_lo, t_hi, rep)
+        log(f"saved {a.out}")
+    else:
+        net, t_lo, t_hi = load_net(a.weights)
+        res = evaluate(net, t_lo, t_hi, a.n, a.seeds, a.ref_factor, log=log)
+        if a.out:
+            with open(a.out, "w") as f:
+                json.dump(res, f, indent=1)
+
+
+if __name__ == "__main__":
+    main()

@@ -207,6 +207,49 @@ const char *gdf_mlp_last_error(void);
  * and where t_lo <= p < t_hi if KXRCF flags the cell. */
 int gdf_set_indicator(GdfHandle *h, GdfMlp *m, float t_lo, float t_hi);
 
+/* ---- ensemble (no counterpart in the reference, which runs one problem
+ * per process) -------------------------------------------------------------
+ * n independent problems, each with its own GdfConfig (grid size, domain,
+ * flux, limiter settings), advanced together: one persistent cooperative
+ * kernel per RK3 stage over all instances, a step captured as one CUDA
+ * graph. Each instance takes its own dt (its own calculate_dt maximum) and
+ * stops at its own tend; its trajectory is value for value the one a
+ * GdfHandle with the same config computes. Instance i's arrays have the
+ * reference extents of its config. */
+typedef struct GdfEnsemble GdfEnsemble;
+int gdf_ens_create(const GdfConfig *cfgs, int32_t n, GdfEnsemble **out);
+int gdf_ens_destroy(GdfEnsemble *e);
+int gdf_ens_upload(GdfEnsemble *e, int32_t i, const double *uh, const double *bx, const double *by);
+int gdf_ens_download(GdfEnsemble *e, int32_t i, double *uh, double *bx, double *by);
+/* every instance must have detector GDF_DETECT_LEARNED; one network for all */
+int gdf_ens_set_indicator(GdfEnsemble *e, GdfMlp *m, float t_lo, float t_hi);
+/* t and tend of instance i (i = -1: all); resets its status */
+int gdf_ens_set_time(GdfEnsemble *e, int32_t i, double t, double tend);
+int gdf_ens_get_time(GdfEnsemble *e, int32_t i, double *t, double *dt, int64_t *steps);
+/* RK3.f90:8-12 for every instance (t = 0, tend unbounded until set) */
+int gdf_ens_prepare(GdfEnsemble *e);
+/* `steps` ensemble steps: every instance with t < tend takes one step per
+ * ensemble step. cell_updates = sum over instances of nx*ny*(steps taken),
+ * n_active = instances still short of their tend, device_ms = CUDA-event
+ * time of the replays (any may be NULL). GDF_ERR_NUMERIC names the first
+ * failing instance; GDF_ERR_TIMEOUT if a grid barrier gave up. */
+int gdf_ens_advance(GdfEnsemble *e, int32_t steps, int64_t *cell_updates, int32_t *n_active,
+                    double *device_ms);
+/* Tile shape: resident blocks per SM (0 = the occupancy limit), items per
+ * thread of the face / vertex / set_bc / mode tiles (a warp takes 32x that
+ * many faces), cells per thread of the residual tiles (a block 64x). */
+int gdf_ens_set_tiles(GdfEnsemble *e, int32_t ctas_per_sm, int32_t face_per_thread,
+                      int32_t cell_per_thread);
+int gdf_ens_get_tiles(GdfEnsemble *e, int32_t *ctas_per_sm, int32_t *face_per_thread,
+                      int32_t *cell_per_thread, int32_t *grid, int32_t *graph);
+/* Autotuner: times `steps` steps of each of the 36 candidate tile shapes
+ * (blocks per SM 1..4 x face items 1,2,4 x cells 1,2,4) from the current
+ * state, restoring the state after every trial, and keeps the fastest.
+ * ms_out (36 floats, or NULL) receives ms per step, -1 where not resident. */
+int gdf_ens_tune(GdfEnsemble *e, int32_t steps, float *ms_out);
+int64_t gdf_ens_kernel_launches(GdfEnsemble *e);
+const char *gdf_ens_last_error(void);
+
 /* Lh (as gdf_lh) on caller-owned DEVICE buffers, allocating no device
  * memory: d_uh and d_du are device pointers with the uh extents of the
  * config (d_du receives du, ghost and unused entries 0). No counterpart in
