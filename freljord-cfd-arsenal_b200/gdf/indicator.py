@@ -6,24 +6,27 @@ Data. Seeded MHD blasts (centre uniform in [-0.2, 0.2]^2, radius 0.1,
 rho = 1, outer pressure 0.1, inner/outer pressure ratio log-uniform in
 [1e2, 1e4], |B| uniform in [0, 100/sqrt(4 pi)] at a uniform angle, gamma
 1.4, HLLD, KXRCF + TVB + positivity limiter) run on the device with the
-plain solver. At sampled steps the stage-1 pre-limit state u + dt L(u) is
-formed (Lh, LhEz and calculate_dt through the C ABI), and each interior cell
-gets its 90 inputs (gdf_features) and the label
+plain solver. At sampled steps the state u before the step is kept, its
+stage-1 pre-limit state u + dt L(u) is formed (Lh, LhEz and calculate_dt
+through the C ABI, value for value the step's own), each interior cell
+gets its 90 inputs (gdf_features of that state), and the step is then
+taken by the plain solver, whose flag word gives the label
 
-    y = KXRCF flags the cell (per stage, not sticky)
-        AND the characteristic TVB limiter changes it (detector ALL),
+    y = the plain method changed the cell at stage 1
+        (sticky KXRCF flag AND the characteristic TVB limiter modified it).
 
-i.e. the cells where the reference's trigger leads to a modified solution.
-Smooth cells (y = 0) far outnumber the rest and are subsampled.
+A gate that fires exactly on these cells reproduces the plain step: a
+gated cell that TVB leaves alone and an ungated cell are the same.
 
 Gate. With thresholds t_lo <= t_hi the limiter runs where p >= t_hi, not
-where p < t_lo, and KXRCF decides in between; (0, 0) is the all-cells
-limiter and (0, > 1) is per-stage KXRCF exactly. The positivity limiter and
-the divergence-free reconstruction always run unchanged in FP64.
+where p < t_lo, and KXRCF (per stage) decides in between; (0, 0) is the
+all-cells limiter and (0, > 1) is per-stage KXRCF exactly. The positivity
+limiter and the divergence-free reconstruction always run unchanged in
+FP64.
 
 Run as a module:
-    python -m gdf.indicator train --out weights.npy   (data, training, thresholds)
-    python -m gdf.indicator eval --weights weights.npy --n 512 --seeds 1001 1002
+    python -m gdf.indicator train --out weights.npz   (data, training, thresholds)
+    python -m gdf.indicator eval --weights weights.npz --n 512 --seeds 1001 1002
 """
 from __future__ import annotations
 
@@ -100,9 +103,9 @@ class Labeller:
         return X, change & kx, kx, change
 
 
-def collect(n: int, seeds, samples_per_run: int = 6, neg_keep: float = 0.15, exact: bool = True, log=None):
-    """Labelled cells from seeded blasts of n x n cells: every positive and a
-    `neg_keep` share of the negatives (seeded)."""
+def collect(n: int, seeds, samples_per_run: int = 8, keep: float = 0.2, exact: bool = True, log=None):
+    """Labelled cells from seeded blasts of n x n cells along the plain
+    trajectory: a seeded `keep` share of each sample's cells."""
     Xs, ys = [], []
     lab = None
     for seed in seeds:
@@ -113,21 +116,33 @@ def collect(n: int, seeds, samples_per_run: int = 6, neg_keep: float = 0.15, exa
         s.upload(uh, bx, by)
         s.prepare()
         rng = np.random.default_rng(10_000 + seed)
-        for k in range(samples_per_run):
-            t_k = tend * (k + 0.5) / samples_per_run
-            s.advance(t_k, 10**7)
-            u, b, c = s.download()
-            X, y, _, _ = lab.sample(u, b, c)
-            keep = y | (rng.random(y.size) < neg_keep)
-            Xs.append(X[keep])
-            ys.append(y[keep].astype(np.float32))
+        try:
+            for k in range(samples_per_run):
+                s.advance(tend * (k + 0.5) / samples_per_run, 10**7)
+                X, y = plain_step_sample(s, lab, tend)
+                sel = rng.random(y.size) < keep
+                Xs.append(X[sel])
+                ys.append(y[sel].astype(np.float32))
+        except Exception as e:   # a run the plain method cannot finish keeps its samples so far
+            if log:
+                log(f"seed {seed}: stopped ({e})")
         s.close()
         if log:
             log(f"seed {seed}: {sum(len(v) for v in ys)} samples so far, positives {sum(v.sum() for v in ys):.0f}")
     return np.concatenate(Xs), np.concatenate(ys)
 
 
-def choose_thresholds(p, y, miss: float = 0.002, fp: float = 0.002):
+def plain_step_sample(s: Solver, lab: Labeller, tend: float):
+    """Inputs of the stage-1 pre-limit state of s's current state and the
+    plain method's stage-1 change flags, taking that step on s."""
+    u, b, c = s.download()
+    ui, _, _ = lab.prelimit(u, b, c)
+    X = lab.s_all.features(ui)
+    _, _, f = s.step(tend)
+    return X, (f.ravel() & 0xFF) != 0
+
+
+def choose_thresholds(p, y, miss: float = 0.01, fp: float = 0.02):
     """t_lo: the largest threshold missing at most `miss` of the positives
     below it; t_hi: the smallest threshold passing at most `fp` of the
     negatives above it (t_hi >= t_lo)."""
@@ -211,36 +226,44 @@ def run(n: int, seed: int, net=None, t_lo=0.5, t_hi=0.5, exact: bool = True, ten
     return u, steps, ms / max(steps, 1), gated / max(chunks, 1)
 
 
-def restrict_means(u_fine, n):
-    """Cell means of an (2n)^2 state averaged onto the n^2 grid."""
-    r = u_fine[:, 0, 1:-1, 1:-1]
-    return 0.25 * (r[:, 0::2, 0::2] + r[:, 1::2, 0::2] + r[:, 0::2, 1::2] + r[:, 1::2, 1::2])
+def fine_reference(n: int, seed: int, factor: int = 2, cache: str | None = None, exact: bool = True):
+    """Cell-mean density of the plain run on a grid `factor` times finer,
+    averaged onto n x n (cached as .npy under `cache`)."""
+    path = os.path.join(cache, f"blast_ref_{n}x{factor}_seed{seed}.npy") if cache else None
+    if path and os.path.exists(path):
+        return np.load(path)
+    u_f, _, _, _ = run(n * factor, seed, exact=exact)
+    r = u_f[0, 0, 1:-1, 1:-1]
+    k = factor
+    rho = r.reshape(n, k, n, k).mean(axis=(1, 3))
+    if path:
+        os.makedirs(cache, exist_ok=True)
+        np.save(path, rho)
+    return rho
 
 
 def evaluate(net, t_lo, t_hi, n: int, seeds, ref_factor: int = 2, samples: int = 4, exact: bool = True,
-             log=None):
+             cache: str | None = None, log=None):
     """Held-out evaluation: L1 density error of the plain and learned runs
     against a plain run on a grid ref_factor times finer, the L1 difference
-    learned vs plain, and the gate's miss / false-positive rates against the
-    labels along the plain trajectory."""
+    learned vs plain, the throughput of both, and the gate's miss /
+    false-positive rates against the plain method's stage-1 decisions along
+    the plain trajectory."""
     out = []
     for seed in seeds:
         u_p, st_p, ms_p, g_p = run(n, seed, None, exact=exact)
         u_l, st_l, ms_l, g_l = run(n, seed, net, t_lo, t_hi, exact=exact)
         rho_p, rho_l = u_p[0, 0, 1:-1, 1:-1], u_l[0, 0, 1:-1, 1:-1]
-        h2 = 1.0 / (n * n)
         rec = {"seed": seed, "n": n, "steps_plain": st_p, "steps_learned": st_l,
                "ms_per_step_plain": ms_p, "ms_per_step_learned": ms_l,
-               "gated_per_step_plain": g_p, "gated_per_step_learned": g_l,
-               "l1_rho_learned_vs_plain": float(np.abs(rho_l - rho_p).sum() * h2),
-               "l1_rho_plain": float(np.abs(rho_p).sum() * h2)}
+               "run_ms_plain": ms_p * st_p, "run_ms_learned": ms_l * st_l,
+               "flagged_per_step_plain": g_p, "flagged_per_step_learned": g_l,
+               "l1_rho_learned_vs_plain": float(np.abs(rho_l - rho_p).mean() / np.abs(rho_p).mean())}
         if ref_factor:
-            u_f, _, _, _ = run(n * ref_factor, seed, None, exact=exact)
-            rho_f = restrict_means(u_f, n)[0] if ref_factor == 2 else None
-            rec["l1_err_plain"] = float(np.abs(rho_p - rho_f).sum() * h2)
-            rec["l1_err_learned"] = float(np.abs(rho_l - rho_f).sum() * h2)
+            rho_f = fine_reference(n, seed, ref_factor, cache, exact)
+            rec["l1_err_plain"] = float(np.abs(rho_p - rho_f).mean())
+            rec["l1_err_learned"] = float(np.abs(rho_l - rho_f).mean())
             rec["l1_err_ratio"] = rec["l1_err_learned"] / rec["l1_err_plain"]
-        # gate quality along the plain trajectory
         cfg, tend, uh, bx, by = blast_setup(n, seed, exact=exact)
         lab = Labeller(cfg, exact)
         s = Solver(cfg, exact)
@@ -249,7 +272,12 @@ def evaluate(net, t_lo, t_hi, n: int, seeds, ref_factor: int = 2, samples: int =
         tp = fn = fp = tn = band = 0
         for k in range(samples):
             s.advance(tend * (k + 0.5) / samples, 10**7)
-            X, y, kx, _ = lab.sample(*s.download())
+            u, b, c = s.download()
+            ui, bi, ci = lab.prelimit(u, b, c)
+            X = lab.s_all.features(ui)
+            kx = (lab.s_kx.limit(ui.copy(), bi.copy(), ci.copy()).ravel() & GATE_BIT) != 0
+            _, _, f = s.step(tend)
+            y = (f.ravel() & 0xFF) != 0
             p = net.predict(X)
             gate = (p >= t_hi) | ((p >= t_lo) & kx)
             tp += int(np.sum(gate & y)); fn += int(np.sum(~gate & y))
@@ -257,8 +285,9 @@ def evaluate(net, t_lo, t_hi, n: int, seeds, ref_factor: int = 2, samples: int =
             band += int(np.sum((p >= t_lo) & (p < t_hi)))
         s.close()
         rec.update({"miss_rate": fn / max(tp + fn, 1), "false_positive_rate": fp / max(fp + tn, 1),
-                    "band_share": band / max(tp + fn + fp + tn, 1), "positives": tp + fn,
-                    "cells_sampled": tp + fn + fp + tn})
+                    "gated_share": (tp + fp) / max(tp + fn + fp + tn, 1),
+                    "positive_share": (tp + fn) / max(tp + fn + fp + tn, 1),
+                    "band_share": band / max(tp + fn + fp + tn, 1), "cells_sampled": tp + fn + fp + tn})
         if log:
             log(json.dumps(rec))
         out.append(rec)
@@ -271,8 +300,8 @@ def main(argv=None):
     t = sub.add_parser("train")
     t.add_argument("--n", type=int, default=256)
     t.add_argument("--seeds", type=int, default=24)
-    t.add_argument("--samples-per-run", type=int, default=6)
-    t.add_argument("--neg-keep", type=float, default=0.15)
+    t.add_argument("--samples-per-run", type=int, default=8)
+    t.add_argument("--keep", type=float, default=0.2)
     t.add_argument("--epochs", type=int, default=12)
     t.add_argument("--out", default=WEIGHTS)
     e = sub.add_parser("eval")
@@ -281,20 +310,21 @@ def main(argv=None):
     e.add_argument("--seeds", type=int, nargs="+", default=[1001, 1002])
     e.add_argument("--ref-factor", type=int, default=2)
     e.add_argument("--out", default=None)
+    e.add_argument("--cache", default=None, help="directory for the fine-grid reference densities")
     a = ap.parse_args(argv)
     log = lambda m: print(m, flush=True)  # noqa: E731
     if a.cmd == "train":
         t0 = time.time()
-        X, y = collect(a.n, range(a.seeds), a.samples_per_run, a.neg_keep, log=log)
+        X, y = collect(a.n, range(a.seeds), a.samples_per_run, a.keep, log=log)
         log(f"collected {len(y)} cells ({int(y.sum())} positive) in {time.time() - t0:.1f} s")
         net, t_lo, t_hi, rep = train(X, y, epochs=a.epochs, log=log)
         rep.update({"grid": a.n, "train_seeds": a.seeds, "samples_per_run": a.samples_per_run,
-                    "neg_keep": a.neg_keep})
+                    "keep": a.keep})
         save(a.out, net, t_lo, t_hi, rep)
         log(f"saved {a.out}")
     else:
         net, t_lo, t_hi = load_net(a.weights)
-        res = evaluate(net, t_lo, t_hi, a.n, a.seeds, a.ref_factor, log=log)
+        res = evaluate(net, t_lo, t_hi, a.n, a.seeds, a.ref_factor, cache=a.cache, log=log)
         if a.out:
             with open(a.out, "w") as f:
                 json.dump(res, f, indent=1)
