@@ -709,23 +709,29 @@ static __device__ void pp_cell(const Consts& K, double (*m)[NP]) {
     for (int d = 1; d < NP; ++d) m[n][d] = eta * m[n][d];
 }
 
-// One interior cell (item < nx*ny). LEARNED: called by every thread of a
+// One interior cell (item < nx*ny). LIM_INFER: called by every thread of a
 // LIM_BS-thread block on LIM_BS consecutive items (those past nx*ny idle),
 // with lsm the block's LIMIT_SMEM_LEARNED bytes of dynamic shared memory.
-template <bool LEARNED>
+// LM (the detector mode): LIM_PLAIN, the reference's detectors; LIM_INFER,
+// the learned gate with inference (the first stage of a step: the block runs
+// the network on its cells and stores each probability in pnet);
+// LIM_PNET, the learned gate on the step's stored probabilities (stages 2
+// and 3: the network sees the step's stage-1 pre-limit state).
+constexpr int LIM_PLAIN = 0, LIM_INFER = 1, LIM_PNET = 2;
+template <int LM>
 __device__ __forceinline__ void limit_item(const Consts& K, const double* __restrict__ S, double* __restrict__ D,
                                            const double* __restrict__ BX, const double* __restrict__ BY,
                                            int32_t* __restrict__ flags, int32_t* __restrict__ trouble, int stage,
                                            int divfree, Scal* __restrict__ sc, const MlpDev* __restrict__ net,
-                                           const float* __restrict__ QM, float t_lo, float t_hi, long long item,
-                                           unsigned char* lsm) {
+                                           const float* __restrict__ QM, float* __restrict__ pnet,
+                                           float t_lo, float t_hi, long long item, unsigned char* lsm) {
   const bool valid = item < (long long)K.nx * K.ny;
   const int i = valid ? (int)(item % K.nx) + 1 : 1;
   const int j = valid ? (int)(item / K.nx) + 1 : 1;
   const long long c = i + (long long)K.nx2 * j;
   const long long pl = K.plane;
   float p_net = 0.f;
-  if (LEARNED) {
+  if (LM == LIM_INFER) {
     // the learned indicator for the block's 64 cells on the tensor cores
     __nv_bfloat16* Xs = reinterpret_cast<__nv_bfloat16*>(lsm);
     __nv_bfloat16* W1t = Xs + LIM_BS * MLP_LDX;
@@ -733,9 +739,18 @@ __device__ __forceinline__ void limit_item(const Consts& K, const double* __rest
     __nv_bfloat16* H1 = W2t + MLP_H * MLP_LDH;
     float* zz = reinterpret_cast<float*>(H1 + LIM_BS * MLP_LDH);
     const int tid = threadIdx.x;
-    for (int k = tid; k < MLP_H * MLP_INP; k += LIM_BS) W1t[(k / MLP_INP) * MLP_LDX + k % MLP_INP] = net->W1t[k];
-    for (int k = tid; k < MLP_H * MLP_H; k += LIM_BS) W2t[(k / MLP_H) * MLP_LDH + k % MLP_H] = net->W2t[k];
-    float f[NFEAT];
+    // weights: 16-byte rows pieces (W1t rows 12 x 16 B, W2t rows 8 x 16 B)
+    const uint4* g1 = reinterpret_cast<const uint4*>(net->W1t);
+    const uint4* g2 = reinterpret_cast<const uint4*>(net->W2t);
+    for (int k = tid; k < MLP_H * (MLP_INP / 8); k += LIM_BS) {
+      const int r = k / (MLP_INP / 8), q = k % (MLP_INP / 8);
+      *reinterpret_cast<uint4*>(W1t + r * MLP_LDX + 8 * q) = g1[k];
+    }
+    for (int k = tid; k < MLP_H * (MLP_H / 8); k += LIM_BS) {
+      const int r = k / (MLP_H / 8), q = k % (MLP_H / 8);
+      *reinterpret_cast<uint4*>(W2t + r * MLP_LDH + 8 * q) = g2[k];
+    }
+    float f[MLP_INP];
     if (valid) {
       gather_features(K, QM, c, f);
     } else {
@@ -743,10 +758,26 @@ __device__ __forceinline__ void limit_item(const Consts& K, const double* __rest
       for (int k = 0; k < NFEAT; ++k) f[k] = 0.f;
     }
 #pragma unroll
-    for (int k = 0; k < MLP_INP; ++k) Xs[tid * MLP_LDX + k] = __float2bfloat16_rn(k < NFEAT ? f[k] : 0.f);
+    for (int k = NFEAT; k < MLP_INP; ++k) f[k] = 0.f;
+#pragma unroll
+    for (int q = 0; q < MLP_INP / 8; ++q) {
+      uint4 v;
+      __nv_bfloat162 a = __floats2bfloat162_rn(f[8 * q], f[8 * q + 1]);
+      __nv_bfloat162 b = __floats2bfloat162_rn(f[8 * q + 2], f[8 * q + 3]);
+      __nv_bfloat162 cc = __floats2bfloat162_rn(f[8 * q + 4], f[8 * q + 5]);
+      __nv_bfloat162 d = __floats2bfloat162_rn(f[8 * q + 6], f[8 * q + 7]);
+      v.x = *reinterpret_cast<uint32_t*>(&a);
+      v.y = *reinterpret_cast<uint32_t*>(&b);
+      v.z = *reinterpret_cast<uint32_t*>(&cc);
+      v.w = *reinterpret_cast<uint32_t*>(&d);
+      *reinterpret_cast<uint4*>(Xs + tid * MLP_LDX + 8 * q) = v;
+    }
     __syncthreads();
     mlp_infer_tiles(Xs, W1t, W2t, net->b1, net->b2, net->w3, net->b3, H1, zz, LIM_BS);
     p_net = 1.f / (1.f + expf(-zz[tid]));
+    if (valid) pnet[item] = p_net;
+  } else if (LM == LIM_PNET) {
+    if (valid) p_net = pnet[item];
   }
   if (!valid) return;
   double m[NE][NP];
@@ -762,7 +793,7 @@ __device__ __forceinline__ void limit_item(const Consts& K, const double* __rest
     gate = prev ? true : kxrcf_flag(K, S, c, m, prev);
     trouble[item] = gate ? 1 : 0;
     if (gate) word |= (1 << 24);
-  } else if (LEARNED) {
+  } else if (LM != LIM_PLAIN) {
     // confident network answers decide; KXRCF decides in the uncertain band
     if (p_net >= t_hi) gate = true;
     else if (p_net >= t_lo) gate = kxrcf_flag(K, S, c, m, false);

@@ -61,6 +61,7 @@ struct EnsInst {
   double *Fxh, *Fyh, *EzRL, *EzUD, *EzV;
   int32_t *flags, *trouble;
   float* QM;
+  float* pnet;
 };
 
 struct EnsSync {
@@ -155,12 +156,12 @@ __device__ __forceinline__ void phase_bc(const EnsArgs& A, int kind, int zeroB) 
   });
 }
 
-template <bool LEARNED>
+template <int LM>
 __device__ __forceinline__ void phase_limit(const EnsArgs& A, int stage, unsigned char* sm) {
   for_tiles<true>(A, EK_LIM, [&](int, const EnsInst& I, const Consts& K, long long base, int) {
-    limit_item<LEARNED>(K, I.UI, I.U, I.BX, I.BY, I.flags, I.trouble, stage, K.faceb ? 0 : 1, I.sc, A.net, I.QM,
-                        A.t_lo, A.t_hi, base + threadIdx.x, sm);
-    if (LEARNED) __syncthreads();
+    limit_item<LM>(K, I.UI, I.U, I.BX, I.BY, I.flags, I.trouble, stage, K.faceb ? 0 : 1, I.sc, A.net, I.QM, I.pnet,
+                   A.t_lo, A.t_hi, base + threadIdx.x, sm);
+    if (LM == LIM_INFER) __syncthreads();
   });
 }
 
@@ -289,7 +290,7 @@ __global__ void __launch_bounds__(ENS_BS) k_ens_stage(const __grid_constant__ En
     });
     if (!ens_barrier(A, &s_ok)) return;
   }
-  if (LEARNED) {
+  if (LEARNED && stage <= 1) {   // the network sees the stage-1 pre-limit state
     for_tiles<true>(A, EK_QM, [&](int, const EnsInst& I, const Consts& K, long long base, int per) {
       for (int k = threadIdx.x; k < per; k += ENS_BS) {
         const long long item = base + k;
@@ -298,7 +299,9 @@ __global__ void __launch_bounds__(ENS_BS) k_ens_stage(const __grid_constant__ En
     });
     if (!ens_barrier(A, &s_ok)) return;
   }
-  phase_limit<LEARNED>(A, stage == 0 ? 1 : stage, sm);
+  if (!LEARNED) phase_limit<LIM_PLAIN>(A, stage == 0 ? 1 : stage, sm);
+  else if (stage <= 1) phase_limit<LIM_INFER>(A, stage == 0 ? 1 : stage, sm);
+  else phase_limit<LIM_PNET>(A, stage, sm);
   if (!ens_barrier(A, &s_ok)) return;
   if (A.any_faceb && !phase_faceb(A, &s_ok)) return;
   // RK3.f90:97 / :123 set_bc after stages 1 and 2; after stage 3 (and the
@@ -538,7 +541,7 @@ int gdf_ens_destroy(GdfEnsemble* e) {
   for (auto& b : e->in) {
     EnsInst& d = b.d;
     void* bufs[] = {d.U, d.U0, d.UI, d.BX, d.BX0, d.BXI, d.BY, d.BY0, d.BYI, d.Fxh, d.Fyh, d.EzRL, d.EzUD,
-                    d.EzV, d.flags, d.trouble, d.QM, b.Us, b.BXs, b.BYs, b.Ts};
+                    d.EzV, d.flags, d.trouble, d.QM, d.pnet, b.Us, b.BXs, b.BYs, b.Ts};
     for (void* p : bufs)
       if (p) cudaFree(p);
   }
@@ -664,6 +667,7 @@ int gdf_ens_set_indicator(GdfEnsemble* e, GdfMlp* m, float t_lo, float t_hi) {
   for (int i = 0; i < e->n; ++i) {
     EnsInst& d = e->in[i].d;
     if (!d.QM) ECK(cudaMalloc((void**)&d.QM, (size_t)18 * e->in[i].K.plane * sizeof(float)));
+    if (!d.pnet) ECK(cudaMalloc((void**)&d.pnet, (size_t)e->in[i].K.nx * e->in[i].K.ny * sizeof(float)));
     hi[i] = d;
   }
   ECK(cudaMemcpy(e->dInst, hi.data(), (size_t)e->n * sizeof(EnsInst), cudaMemcpyHostToDevice));

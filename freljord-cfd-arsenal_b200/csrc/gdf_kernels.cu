@@ -109,17 +109,17 @@ __global__ void k_features(const __grid_constant__ Consts K, const float* __rest
   for (int k = 0; k < NFEAT; ++k) X[item * NFEAT + k] = f[k];
 }
 
-template <bool LEARNED>
+template <int LM>
 __global__ void __launch_bounds__(LIM_BS) k_limit(const __grid_constant__ Consts K, const double* __restrict__ S,
                                                   double* __restrict__ D, const double* __restrict__ BX,
                                                   const double* __restrict__ BY, int32_t* __restrict__ flags,
                                                   int32_t* __restrict__ trouble, int stage, int divfree,
                                                   const Scal* __restrict__ gate_sc, Scal* __restrict__ sc,
                                                   const MlpDev* __restrict__ net, const float* __restrict__ QM,
-                                                  float t_lo, float t_hi) {
+                                                  float* __restrict__ pnet, float t_lo, float t_hi) {
   extern __shared__ __align__(16) unsigned char lsm[];
   if (gate_sc && !gate_sc->active) return;
-  limit_item<LEARNED>(K, S, D, BX, BY, flags, trouble, stage, divfree, sc, net, QM, t_lo, t_hi, gtid(), lsm);
+  limit_item<LM>(K, S, D, BX, BY, flags, trouble, stage, divfree, sc, net, QM, pnet, t_lo, t_hi, gtid(), lsm);
 }
 
 __global__ void k_faceb_limit(const __grid_constant__ Consts K, const double* __restrict__ S,
@@ -292,6 +292,7 @@ struct GdfHandle {
   double *Fxh = nullptr, *Fyh = nullptr, *EzRL = nullptr, *EzUD = nullptr, *EzV = nullptr;
   double *part = nullptr;
   float* QM = nullptr;       // learned-indicator feature modes (18 per cell)
+  float* pnet = nullptr;     // learned-indicator probability per interior cell (this step)
   MlpDev* net = nullptr;     // learned-indicator network (device copy)
   float t_lo = 0.5f, t_hi = 0.5f;
   int32_t *flags = nullptr, *trouble = nullptr;
@@ -492,21 +493,30 @@ static int launch_limit(GdfHandle* h, const double* S, double* D, int stage, con
   const long long ncell = (long long)K.nx * K.ny;
   const int fused_divfree = K.faceb ? 0 : 1;
   size_t smem = 0;
+  // the network runs at the first stage of a step (and at the start-up
+  // limiting); stages 2 and 3 reuse its probabilities
+  const int infer = stage <= 1 ? 1 : 0;
   if (K.detector == GDF_DETECT_LEARNED) {
     if (!h->net || !h->QM) return fail(GDF_ERR_STATE, "detector GDF_DETECT_LEARNED needs gdf_set_indicator first");
-    int rq = run_kernel(h, GDF_K_LIMIT, [&] { k_qmodes<<<nblk(K.plane, 128), 128, 0, h->st>>>(K, S, h->QM); });
-    if (rq) return rq;
-    smem = LIMIT_SMEM_LEARNED;
+    if (infer) {
+      int rq = run_kernel(h, GDF_K_LIMIT, [&] { k_qmodes<<<nblk(K.plane, 128), 128, 0, h->st>>>(K, S, h->QM); });
+      if (rq) return rq;
+      smem = LIMIT_SMEM_LEARNED;
+    }
   }
   int rc0 = run_kernel(h, GDF_K_LIMIT, [&] {
-    if (K.detector == GDF_DETECT_LEARNED)
-      k_limit<true><<<nblk(ncell, LIM_BS), LIM_BS, smem, h->st>>>(K, S, D, h->BX, h->BY, h->flags, h->trouble, stage,
-                                                                  fused_divfree, sc_gate, h->sc, h->net, h->QM,
-                                                                  h->t_lo, h->t_hi);
+    const unsigned nb = nblk(ncell, LIM_BS);
+    if (K.detector == GDF_DETECT_LEARNED && infer)
+      k_limit<LIM_INFER><<<nb, LIM_BS, smem, h->st>>>(K, S, D, h->BX, h->BY, h->flags, h->trouble, stage,
+                                                      fused_divfree, sc_gate, h->sc, h->net, h->QM, h->pnet, h->t_lo,
+                                                      h->t_hi);
+    else if (K.detector == GDF_DETECT_LEARNED)
+      k_limit<LIM_PNET><<<nb, LIM_BS, 0, h->st>>>(K, S, D, h->BX, h->BY, h->flags, h->trouble, stage, fused_divfree,
+                                                  sc_gate, h->sc, h->net, h->QM, h->pnet, h->t_lo, h->t_hi);
     else
-      k_limit<false><<<nblk(ncell, LIM_BS), LIM_BS, 0, h->st>>>(K, S, D, h->BX, h->BY, h->flags, h->trouble, stage,
-                                                                fused_divfree, sc_gate, h->sc, nullptr, nullptr,
-                                                                0.f, 0.f);
+      k_limit<LIM_PLAIN><<<nb, LIM_BS, 0, h->st>>>(K, S, D, h->BX, h->BY, h->flags, h->trouble, stage,
+                                                   fused_divfree, sc_gate, h->sc, nullptr, nullptr, nullptr, 0.f,
+                                                   0.f);
   });
   if (rc0) return rc0;
   if (K.faceb) {
@@ -695,6 +705,7 @@ int gdf_destroy(GdfHandle* h) {
   for (double* p : bufs)
     if (p) cudaFree(p);
   if (h->QM) cudaFree(h->QM);
+  if (h->pnet) cudaFree(h->pnet);
   if (h->net) cudaFree(h->net);
   if (h->flags) cudaFree(h->flags);
   if (h->trouble) cudaFree(h->trouble);
@@ -877,6 +888,7 @@ int gdf_set_indicator(GdfHandle* h, GdfMlp* m, float t_lo, float t_hi) {
   if (!(t_lo <= t_hi)) return fail(GDF_ERR_ARG, "t_lo must not exceed t_hi");
   if (!h->net) CK(cudaMalloc((void**)&h->net, sizeof(MlpDev)));
   if (!h->QM) CK(cudaMalloc((void**)&h->QM, (size_t)QMODES * h->K.plane * sizeof(float)));
+  if (!h->pnet) CK(cudaMalloc((void**)&h->pnet, (size_t)h->K.nx * h->K.ny * sizeof(float)));
   CK(cudaMemcpy(h->net, gdf_mlp_device_params(m), sizeof(MlpDev), cudaMemcpyDeviceToDevice));
   h->t_lo = t_lo;
   h->t_hi = t_hi;
