@@ -294,18 +294,79 @@ def run_reference(args):
 
 
 def run_quick(args):
-    """Warm-up and timed steps only: the command the ncu captures run."""
+    """Warm-up and timed steps only: the commands the ncu captures run.
+
+    --workload rotor           the benchmark workload (rotor 512^2, plain)
+    --workload blast-learned   blast 512^2 with the shipped learned gate
+    --workload ensemble-small  8 instances (64^2..160^2, OT / rotor / blast,
+                               HLLD, learned gate) in the persistent kernels
+    --workload mlp-train       one epoch of indicator training on 65536
+                               synthetic samples (batch 2048)"""
     import gdf
     gdf.set_device(dist_env()[2])
-    cfg, uh, bx, by = make_state(gdf)
-    s = gdf.Solver(cfg, exact=not args.fma)
-    s.upload(uh, bx, by)
-    s.prepare()
+    w = args.workload
+    if w == "rotor":
+        cfg, uh, bx, by = make_state(gdf)
+        s = gdf.Solver(cfg, exact=not args.fma)
+        s.upload(uh, bx, by)
+        s.prepare()
+        if args.warmup:
+            s.advance_timed(1e9, args.warmup)
+        _, n, ms = s.advance_timed(1e9, args.steps)
+        print(json.dumps({"quick": True, "workload": w, "steps": n, "ms_per_step": ms / n,
+                          "value": NX * NY * n / (ms / 1e3)}))
+        s.close()
+        return 0
+    if w == "mlp-train":
+        import numpy as np
+        rng = np.random.default_rng(0)
+        X = rng.normal(0, 1, (65536, gdf.NFEAT)).astype(np.float32)
+        y = (X[:, :8].sum(1) > 1.0).astype(np.float32)
+        m = gdf.Mlp(0)
+        t0 = time.perf_counter()
+        loss = m.train(X, y, epochs=1, batch=2048, lr=1e-3)
+        print(json.dumps({"quick": True, "workload": w, "loss": float(loss[0]),
+                          "seconds": time.perf_counter() - t0}))
+        return 0
+    from gdf.indicator import WEIGHTS, load_net
+    net, lo, hi = load_net(WEIGHTS)
+    if w == "blast-learned":
+        cfg, tend = gdf.problem_config(gdf.PROB_BLAST, 512, 512)
+        cfg.detector = gdf.DETECT_LEARNED
+        s = gdf.Solver(cfg)
+        s.set_indicator(net, lo, hi)
+        s.upload(*gdf.init_data(cfg, gdf.PROB_BLAST))
+        s.prepare()
+        if args.warmup:
+            s.advance_timed(tend, args.warmup)
+        _, n, ms = s.advance_timed(tend, args.steps)
+        print(json.dumps({"quick": True, "workload": w, "steps": n, "ms_per_step": ms / n,
+                          "value": 512 * 512 * n / (ms / 1e3)}))
+        s.close()
+        return 0
+    # ensemble-small
+    items = []
+    for i, (prob, side) in enumerate([(gdf.PROB_ORSZAG_TANG, 64), (gdf.PROB_ROTOR, 96), (gdf.PROB_BLAST, 128),
+                                      (gdf.PROB_ROTOR, 160), (gdf.PROB_BLAST, 64), (gdf.PROB_ORSZAG_TANG, 128),
+                                      (gdf.PROB_ROTOR, 64), (gdf.PROB_BLAST, 96)]):
+        c, te = gdf.problem_config(prob, side, side)
+        c.flux_type = gdf.FLUX_HLLD
+        c.detector = gdf.DETECT_LEARNED
+        c.kxrcf_ck = 1.0
+        items.append((c, prob, te))
+    e = gdf.Ensemble([c for c, _, _ in items])
+    e.set_indicator(net, lo, hi)
+    for i, (c, prob, te) in enumerate(items):
+        e.upload(i, *gdf.init_data(c, prob))
+    e.prepare()
+    for i, (_, _, te) in enumerate(items):
+        e.set_time(i, 0.0, te)
     if args.warmup:
-        s.advance_timed(1e9, args.warmup)
-    _, n, ms = s.advance_timed(1e9, args.steps)
-    print(json.dumps({"quick": True, "steps": n, "ms_per_step": ms / n, "value": NX * NY * n / (ms / 1e3)}))
-    s.close()
+        e.advance(args.warmup)
+    cu, act, ms = e.advance(args.steps)
+    print(json.dumps({"quick": True, "workload": w, "steps": args.steps, "ms_per_step": ms / args.steps,
+                      "value": cu / (ms / 1e3), "tiles": e.tiles()}))
+    e.close()
     return 0
 
 
@@ -439,6 +500,8 @@ def main():
     ap.add_argument("--no-extra", action="store_true", help="skip the learned-indicator and ensemble runs")
     ap.add_argument("--quick", action="store_true", help="timed steps only (for profiler captures)")
     ap.add_argument("--fma", action="store_true", help="with --quick: run the FMA build")
+    ap.add_argument("--workload", default="rotor", choices=["rotor", "blast-learned", "ensemble-small", "mlp-train"],
+                    help="with --quick: what to run")
     args = ap.parse_args()
     if args.quick:
         return run_quick(args)

@@ -291,9 +291,15 @@ def evaluate(net, settings, n: int, seeds, ref_factor: int = 2, samples: int = 4
         P, Y, KX = np.concatenate(P), np.concatenate(Y), np.concatenate(KX)
         rec["positive_share"] = float(Y.mean())
         for name, (lo, hi) in settings.items():
-            u_l, st_l, ms_l, g_l = run(n, seed, net, lo, hi, exact=exact)
-            rho_l = u_l[0, 0, 1:-1, 1:-1]
             gate = (P >= hi) | ((P >= lo) & KX)
+            try:
+                u_l, st_l, ms_l, g_l = run(n, seed, net, lo, hi, exact=exact)
+            except Exception as e:   # the learned run failed (e.g. lost positivity)
+                rec[name] = {"t_lo": lo, "t_hi": hi, "failed": str(e),
+                             "miss_rate": float(np.mean(~gate[Y])) if Y.any() else 0.0,
+                             "false_positive_rate": float(np.mean(gate[~Y])) if (~Y).any() else 0.0}
+                continue
+            rho_l = u_l[0, 0, 1:-1, 1:-1]
             r = {"t_lo": lo, "t_hi": hi, "steps": st_l, "ms_per_step": ms_l, "run_ms": ms_l * st_l,
                  "speedup_run": ms_p * st_p / (ms_l * st_l), "flagged_per_step": g_l,
                  "l1_rho_vs_plain": float(np.abs(rho_l - rho_p).mean() / np.abs(rho_p).mean()),
@@ -326,6 +332,7 @@ def main(argv=None):
     e.add_argument("--seeds", type=int, nargs="+", default=[1001, 1002])
     e.add_argument("--ref-factor", type=int, default=2)
     e.add_argument("--all-settings", action="store_true", help="also every threshold of the training report")
+    e.add_argument("--only", nargs="+", default=None, help="with --all-settings: these report entries only")
     e.add_argument("--out", default=None)
     e.add_argument("--cache", default=None, help="directory for the fine-grid reference densities")
     a = ap.parse_args(argv)
@@ -344,7 +351,8 @@ def main(argv=None):
         if a.all_settings:
             rep = json.loads(str(np.load(a.weights)["report"]))
             for k, v in rep.get("thresholds", {}).items():
-                settings[k] = (v["t_lo"], v["t_hi"])
+                if a.only is None or k in a.only:
+                    settings[k] = (v["t_lo"], v["t_hi"])
         res = evaluate(net, settings, a.n, a.seeds, a.ref_factor, cache=a.cache, log=log)
         if a.out:
             with open(a.out, "w") as f:
