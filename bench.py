@@ -451,9 +451,15 @@ def run_ours(args):
         cpu = cpu_baseline(gdf, args.cpu_steps)
 
     learned = ens = None
-    if not args.no_extra:
-        learned = learned_blast(gdf, args.steps)
-        ens = ensemble_bench(gdf, args.steps)
+    if not args.no_extra and rank == 0 and world == 1:
+        try:
+            learned = learned_blast(gdf, args.steps)
+        except Exception as e:   # reported, not fatal: the headline line still prints
+            learned = {"error": str(e)}
+        try:
+            ens = ensemble_bench(gdf, args.steps)
+        except Exception as e:
+            ens = {"error": str(e)}
 
     if rank == 0:
         line = {
