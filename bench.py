@@ -351,6 +351,7 @@ def run_quick(args):
                                       (gdf.PROB_ROTOR, 64), (gdf.PROB_BLAST, 96)]):
         c, te = gdf.problem_config(prob, side, side)
         c.flux_type = gdf.FLUX_HLLD
+        c.faceb_limiter = 1
         c.detector = gdf.DETECT_LEARNED
         c.kxrcf_ck = 1.0
         items.append((c, prob, te))

@@ -10,7 +10,14 @@
 #include "gdf_kernels.cuh"
 #include "gdf_mlp.cuh"
 
+#include <mutex>
+
 namespace gdf {
+
+// Grid-independent basis tables (one copy per device and module; each
+// translation unit that launches kernels fills its own with
+// upload_basis_once before its first launch on a device).
+static __constant__ Basis c_basis;
 
 // ------------------------------------------------------------ live slots --
 __host__ __device__ constexpr int LI(int n, int d) {
@@ -98,8 +105,8 @@ __device__ __forceinline__ void face_item(const Consts& K, const double* __restr
     for (int d = 0; d < NP; ++d) {
       if (!live_mode(n, d)) continue;
       const long long off = K.plane * (d + 10 * n);
-      const double pl = DIR == 0 ? K.phiGR[g][d] : K.phiGU[g][d];
-      const double pr = DIR == 0 ? K.phiGL[g][d] : K.phiGD[g][d];
+      const double pl = DIR == 0 ? c_basis.phiGR[g][d] : c_basis.phiGU[g][d];
+      const double pr = DIR == 0 ? c_basis.phiGL[g][d] : c_basis.phiGD[g][d];
       a = a + U[off + cL] * pl;
       b = b + U[off + cR] * pr;
     }
@@ -153,10 +160,10 @@ __device__ __forceinline__ void vertex_item(const Consts& K, const double* __res
     for (int d = 0; d < NP; ++d) {
       if (!live_mode(n, d)) continue;
       const long long off = K.plane * (d + 10 * n);
-      a = a + U[off + cRU] * K.phiLD[d];
-      b = b + U[off + cLU] * K.phiRD[d];
-      c = c + U[off + cRD] * K.phiLU[d];
-      e = e + U[off + cLD] * K.phiRU[d];
+      a = a + U[off + cRU] * c_basis.phiLD[d];
+      b = b + U[off + cLU] * c_basis.phiRD[d];
+      c = c + U[off + cRD] * c_basis.phiLU[d];
+      e = e + U[off + cLD] * c_basis.phiRU[d];
     }
     URU[n] = a; ULU[n] = b; URD[n] = c; ULD[n] = e;
   }
@@ -198,7 +205,7 @@ __device__ __forceinline__ void cell_item(const Consts& K, const double* __restr
           double acc = 0.0;
 #pragma unroll
           for (int d = 0; d < NP; ++d)
-            if (live_mode(n, d)) acc = acc + ms[LI(n, d) * CELL_BS + tid] * K.phiG[a][b][d];
+            if (live_mode(n, d)) acc = acc + ms[LI(n, d) * CELL_BS + tid] * c_basis.phiG[a][b][d];
           v[n] = acc;
         }
         const double rho = v[0];
@@ -226,7 +233,7 @@ __device__ __forceinline__ void cell_item(const Consts& K, const double* __restr
         Fy[5] = vv * B1 - u * B2;
         Fy[6] = 0.0;
         Fy[7] = vv * B3 - w * B2;
-        const double coef = 0.25 * K.w[a] * K.w[b];
+        const double coef = 0.25 * c_basis.w[a] * c_basis.w[b];
         // du(d,n) += coef*(Fx*phixG + Fy*phiyG); a product with an exact zero
         // (phixG of modes 1,3,6,10, phiyG of modes 1,2,4,7, Fx(6), Fy(7))
         // contributes +-0 and is left out
@@ -268,14 +275,14 @@ __device__ __forceinline__ void cell_item(const Consts& K, const double* __restr
 #pragma unroll
         for (int g = 0; g < NG; ++g) {
           if (g == 2 && (d == 2 || d == 4 || d == 7 || d == 9)) continue;
-          acc = acc - K.cxs * K.w[g] * (fr[g] * K.phiGR[g][d] - fl[g] * K.phiGL[g][d]);
+          acc = acc - K.cxs * c_basis.w[g] * (fr[g] * c_basis.phiGR[g][d] - fl[g] * c_basis.phiGL[g][d]);
         }
 #pragma unroll
         for (int g = 0; g < NG; ++g) {
           if (g == 2 && (d == 1 || d == 4 || d == 8 || d == 6)) continue;
-          acc = acc - K.cys * K.w[g] * (fu[g] * K.phiGU[g][d] - fd[g] * K.phiGD[g][d]);
+          acc = acc - K.cys * c_basis.w[g] * (fu[g] * c_basis.phiGU[g][d] - fd[g] * c_basis.phiGD[g][d]);
         }
-        du[LI(n, d)] = acc / K.mm[d];
+        du[LI(n, d)] = acc / c_basis.mm[d];
       }
     }
   }
@@ -336,8 +343,8 @@ __device__ __forceinline__ void bface_item(const Consts& K, const double* __rest
     for (int d = 0; d < 3; ++d) {
       double acc = 0.0;
 #pragma unroll
-      for (int g = 0; g < NG; ++g) acc = acc + 0.5 * K.w[g] * EzRL[g * fp + o] * K.EzyG[g][d];
-      dez[d] = (acc - v1 * K.EzU[d] / K.hy + v0 * K.EzD[d] / K.hy) / K.mmE[d];
+      for (int g = 0; g < NG; ++g) acc = acc + 0.5 * c_basis.w[g] * EzRL[g * fp + o] * K.EzyG[g][d];
+      dez[d] = (acc - v1 * c_basis.EzU[d] / K.hy + v0 * c_basis.EzD[d] / K.hy) / c_basis.mmE[d];
     }
     B = BX; B0 = BX0; BI = BXI; dout = dez1;
   } else {
@@ -352,8 +359,8 @@ __device__ __forceinline__ void bface_item(const Consts& K, const double* __rest
     for (int d = 0; d < 3; ++d) {
       double acc = 0.0;
 #pragma unroll
-      for (int g = 0; g < NG; ++g) acc = acc - 0.5 * K.w[g] * EzUD[g * fp + o] * K.EzxG[g][d];
-      dez[d] = (acc + v1 * K.EzR[d] / K.hx - v0 * K.EzL[d] / K.hx) / K.mmE[d];
+      for (int g = 0; g < NG; ++g) acc = acc - 0.5 * c_basis.w[g] * EzUD[g * fp + o] * K.EzxG[g][d];
+      dez[d] = (acc + v1 * c_basis.EzR[d] / K.hx - v0 * c_basis.EzL[d] / K.hx) / c_basis.mmE[d];
     }
     B = BY; B0 = BY0; BI = BYI; dout = dez2;
   }
@@ -526,40 +533,40 @@ static __device__ bool kxrcf_flag(const Consts& K, const double* __restrict__ S,
   if (S[c + 1 + pl * 10] < 0) {  // uh(i+1,j,1,2) < 0: right side inflow
 #pragma unroll 1
     for (int g = 0; g < NG; ++g) {
-      trace8(K, S, c, K.phiGR[g], A);
-      trace8(K, S, c + 1, K.phiGL[g], B);
+      trace8(K, S, c, c_basis.phiGR[g], A);
+      trace8(K, S, c + 1, c_basis.phiGL[g], B);
 #pragma unroll
-      for (int n = 0; n < NE; ++n) I[n] = I[n] + K.hy1 * K.w[g] * (A[n] - B[n]);
+      for (int n = 0; n < NE; ++n) I[n] = I[n] + K.hy1 * c_basis.w[g] * (A[n] - B[n]);
       Lij = Lij + K.hy;
     }
   }
   if (S[c - 1 + pl * 10] > 0) {
 #pragma unroll 1
     for (int g = 0; g < NG; ++g) {
-      trace8(K, S, c, K.phiGL[g], A);
-      trace8(K, S, c - 1, K.phiGR[g], B);
+      trace8(K, S, c, c_basis.phiGL[g], A);
+      trace8(K, S, c - 1, c_basis.phiGR[g], B);
 #pragma unroll
-      for (int n = 0; n < NE; ++n) I[n] = I[n] + K.hy1 * K.w[g] * (A[n] - B[n]);
+      for (int n = 0; n < NE; ++n) I[n] = I[n] + K.hy1 * c_basis.w[g] * (A[n] - B[n]);
       Lij = Lij + K.hy;
     }
   }
   if (S[c + K.nx2 + pl * 20] < 0) {
 #pragma unroll 1
     for (int g = 0; g < NG; ++g) {
-      trace8(K, S, c, K.phiGU[g], A);
-      trace8(K, S, c + K.nx2, K.phiGD[g], B);
+      trace8(K, S, c, c_basis.phiGU[g], A);
+      trace8(K, S, c + K.nx2, c_basis.phiGD[g], B);
 #pragma unroll
-      for (int n = 0; n < NE; ++n) I[n] = I[n] + K.hx1 * K.w[g] * (A[n] - B[n]);
+      for (int n = 0; n < NE; ++n) I[n] = I[n] + K.hx1 * c_basis.w[g] * (A[n] - B[n]);
       Lij = Lij + K.hx;
     }
   }
   if (S[c - K.nx2 + pl * 20] > 0) {
 #pragma unroll 1
     for (int g = 0; g < NG; ++g) {
-      trace8(K, S, c, K.phiGD[g], A);
-      trace8(K, S, c - K.nx2, K.phiGU[g], B);
+      trace8(K, S, c, c_basis.phiGD[g], A);
+      trace8(K, S, c - K.nx2, c_basis.phiGU[g], B);
 #pragma unroll
-      for (int n = 0; n < NE; ++n) I[n] = I[n] + K.hx1 * K.w[g] * (A[n] - B[n]);
+      for (int n = 0; n < NE; ++n) I[n] = I[n] + K.hx1 * c_basis.w[g] * (A[n] - B[n]);
       Lij = Lij + K.hx;
     }
   }
@@ -581,7 +588,7 @@ static __device__ bool kxrcf_flag(const Consts& K, const double* __restrict__ S,
         double v = 0.0;
 #pragma unroll
         for (int d = 0; d < NP; ++d)
-          if (live_mode(n, d)) v = v + m[n][d] * K.phiG[a][b][d];
+          if (live_mode(n, d)) v = v + m[n][d] * c_basis.phiG[a][b][d];
         if (fabs(v) + 1e-12 > uinf[n]) uinf[n] = fabs(v) + 1e-12;
       }
   bool flag = prev;
@@ -616,7 +623,7 @@ __device__ __forceinline__ double pp_spread(const Consts& K, const double (*m)[N
   double b = 0.0;
 #pragma unroll
   for (int d = 1; d < NP; ++d)
-    if (live_mode(n, d)) b = b + fabs(m[n][d]) * K.ppM[d];
+    if (live_mode(n, d)) b = b + fabs(m[n][d]) * c_basis.ppM[d];
   return b * (1.0 + 1e-12) + 1e-12 * fabs(m[n][0]);
 }
 
@@ -641,7 +648,7 @@ static __device__ void pp_cell(const Consts& K, double (*m)[NP]) {
         double rq = 0.0;
 #pragma unroll
         for (int d = 0; d < NP; ++d)
-          if (live_mode(0, d)) rq = rq + m[0][d] * K.phiGLL[s][a][b][d];
+          if (live_mode(0, d)) rq = rq + m[0][d] * c_basis.phiGLL[s][a][b][d];
         const double eta1 = fabs((rb - epsilon) / (rb - rq));
         if (eta1 < 1) eta = eta1;
       }
@@ -685,7 +692,7 @@ static __device__ void pp_cell(const Consts& K, double (*m)[NP]) {
           double acc = 0.0;
 #pragma unroll
           for (int d = 0; d < NP; ++d)
-            if (live_mode(n, d)) acc = acc + m[n][d] * K.phiGLL[s][a][b][d];
+            if (live_mode(n, d)) acc = acc + m[n][d] * c_basis.phiGLL[s][a][b][d];
           uq[n] = acc;
         }
         const double pq = pressure(K.P.gamma, uq);
@@ -1052,6 +1059,24 @@ __device__ __forceinline__ void dt_advance(const Consts& K, double ax, double ay
   sc->t = t;
   sc->active = 1;
   sc->steps += 1;
+}
+
+// Fills this module's c_basis on the current device once (the tables do not
+// depend on the configuration). Returns a cudaError_t.
+static inline cudaError_t upload_basis_once(const Consts& K) {
+  static std::mutex mu;
+  static bool done[256] = {false};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 256) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(mu);
+  if (done[dev]) return cudaSuccess;
+  Basis B;
+  basis_of(K, B);
+  e = cudaMemcpyToSymbol(c_basis, &B, sizeof(Basis));
+  if (e == cudaSuccess) done[dev] = true;
+  return e;
 }
 
 }  // namespace gdf

@@ -85,6 +85,44 @@ struct EnsArgs {
   int total[EK_N];                // tiles
 };
 
+// The per-item bodies are called, not inlined, from the persistent kernel:
+// inlined into one kernel their live ranges add up to a 1.4 KB stack frame
+// whose spills went to DRAM; as calls each keeps the register allocation it
+// has in its own single-problem kernel.
+__device__ __noinline__ void call_face_x(const Consts& K, const double* U, double* F, double* Ez, long long item) {
+  face_item<0>(K, U, F, Ez, item);
+}
+__device__ __noinline__ void call_face_y(const Consts& K, const double* U, double* F, double* Ez, long long item) {
+  face_item<1>(K, U, F, Ez, item);
+}
+__device__ __noinline__ void call_vertex(const Consts& K, const double* U, double* EzV, long long item) {
+  vertex_item(K, U, EzV, item);
+}
+extern __shared__ __align__(16) unsigned char ens_sm[];   // the stage kernel's dynamic shared memory
+__device__ __noinline__ void call_cell(const Consts& K, const double* U, double* U0, double* UI, const double* Fxh,
+                                       const double* Fyh, const Scal* sc, int stage, long long item) {
+  cell_item(K, U, U0, UI, Fxh, Fyh, nullptr, sc, stage, item, reinterpret_cast<double*>(ens_sm));
+}
+__device__ __noinline__ void call_bface(const Consts& K, const double* EzRL, const double* EzUD, const double* EzV,
+                                        double* BX, double* BX0, double* BXI, double* BY, double* BY0, double* BYI,
+                                        const Scal* sc, int stage, long long item) {
+  bface_item(K, EzRL, EzUD, EzV, BX, BX0, BXI, BY, BY0, BYI, nullptr, nullptr, sc, stage, item);
+}
+__device__ __noinline__ void call_qmodes(const Consts& K, const double* S, float* QM, long long item) {
+  qmodes_item(K, S, QM, item);
+}
+template <int LM>
+__device__ __noinline__ void call_limit(const Consts& K, const double* S, double* D, const double* BX, const double* BY,
+                                        int32_t* flags, int32_t* trouble, int stage, int divfree, Scal* sc,
+                                        const MlpDev* net, const float* QM, float* pnet, float t_lo, float t_hi,
+                                        long long item) {
+  limit_item<LM>(K, S, D, BX, BY, flags, trouble, stage, divfree, sc, net, QM, pnet, t_lo, t_hi, item, ens_sm);
+}
+__device__ __noinline__ void call_dt(const Consts& K, const double* U, long long item, double& ax, double& ay,
+                                     Scal* sc) {
+  dt_cell_speeds(K, U, item, ax, ay, sc);
+}
+
 __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -157,10 +195,10 @@ __device__ __forceinline__ void phase_bc(const EnsArgs& A, int kind, int zeroB) 
 }
 
 template <int LM>
-__device__ __forceinline__ void phase_limit(const EnsArgs& A, int stage, unsigned char* sm) {
+__device__ __forceinline__ void phase_limit(const EnsArgs& A, int stage) {
   for_tiles<true>(A, EK_LIM, [&](int, const EnsInst& I, const Consts& K, long long base, int) {
-    limit_item<LM>(K, I.UI, I.U, I.BX, I.BY, I.flags, I.trouble, stage, K.faceb ? 0 : 1, I.sc, A.net, I.QM, I.pnet,
-                   A.t_lo, A.t_hi, base + threadIdx.x, sm);
+    call_limit<LM>(K, I.UI, I.U, I.BX, I.BY, I.flags, I.trouble, stage, K.faceb ? 0 : 1, I.sc, A.net, I.QM, I.pnet,
+                   A.t_lo, A.t_hi, base + threadIdx.x);
     if (LM == LIM_INFER) __syncthreads();
   });
 }
@@ -189,7 +227,6 @@ __device__ __forceinline__ bool phase_faceb(const EnsArgs& A, int* s_ok) {
 // RK3.f90:8-12.
 template <bool LEARNED>
 __global__ void __launch_bounds__(ENS_BS) k_ens_stage(const __grid_constant__ EnsArgs A, int stage) {
-  extern __shared__ __align__(16) unsigned char sm[];
   __shared__ int s_ok;
   __shared__ double s_x[ENS_BS], s_y[ENS_BS];
   if (A.sync->err) return;
@@ -214,7 +251,7 @@ __global__ void __launch_bounds__(ENS_BS) k_ens_stage(const __grid_constant__ En
       double ax = 0.0, ay = 0.0;
       for (int k = threadIdx.x; k < per; k += ENS_BS) {
         const long long item = base + k;
-        if (item < n) dt_cell_speeds(K, I.U, item, ax, ay, I.sc);
+        if (item < n) call_dt(K, I.U, item, ax, ay, I.sc);
       }
       __syncthreads();
       s_x[threadIdx.x] = ax;
@@ -254,20 +291,20 @@ __global__ void __launch_bounds__(ENS_BS) k_ens_stage(const __grid_constant__ En
       const long long n = face_items<0>(K);
       for (int k = threadIdx.x; k < per; k += ENS_BS) {
         const long long item = base + k;
-        if (item < n) face_item<0>(K, I.U, I.Fxh, I.EzRL, item);
+        if (item < n) call_face_x(K, I.U, I.Fxh, I.EzRL, item);
       }
     });
     for_tiles<true>(A, EK_FY, [&](int, const EnsInst& I, const Consts& K, long long base, int per) {
       const long long n = face_items<1>(K);
       for (int k = threadIdx.x; k < per; k += ENS_BS) {
         const long long item = base + k;
-        if (item < n) face_item<1>(K, I.U, I.Fyh, I.EzUD, item);
+        if (item < n) call_face_y(K, I.U, I.Fyh, I.EzUD, item);
       }
     });
     for_tiles<true>(A, EK_VX, [&](int, const EnsInst& I, const Consts& K, long long base, int per) {
       for (int k = threadIdx.x; k < per; k += ENS_BS) {
         const long long item = base + k;
-        if (item < K.vplane) vertex_item(K, I.U, I.EzV, item);
+        if (item < K.vplane) call_vertex(K, I.U, I.EzV, item);
       }
     });
     if (!ens_barrier(A, &s_ok)) return;
@@ -276,7 +313,7 @@ __global__ void __launch_bounds__(ENS_BS) k_ens_stage(const __grid_constant__ En
       for (int k = threadIdx.x; k < per; k += ENS_BS) {
         const long long item = base + k;
         if (item < K.plane)
-          cell_item(K, I.U, I.U0, I.UI, I.Fxh, I.Fyh, nullptr, I.sc, stage, item, reinterpret_cast<double*>(sm));
+          call_cell(K, I.U, I.U0, I.UI, I.Fxh, I.Fyh, I.sc, stage, item);
       }
     });
     for_tiles<true>(A, EK_BF, [&](int, const EnsInst& I, const Consts& K, long long base, int per) {
@@ -284,8 +321,7 @@ __global__ void __launch_bounds__(ENS_BS) k_ens_stage(const __grid_constant__ En
       for (int k = threadIdx.x; k < per; k += ENS_BS) {
         const long long item = base + k;
         if (item < n)
-          bface_item(K, I.EzRL, I.EzUD, I.EzV, I.BX, I.BX0, I.BXI, I.BY, I.BY0, I.BYI, nullptr, nullptr, I.sc,
-                     stage, item);
+          call_bface(K, I.EzRL, I.EzUD, I.EzV, I.BX, I.BX0, I.BXI, I.BY, I.BY0, I.BYI, I.sc, stage, item);
       }
     });
     if (!ens_barrier(A, &s_ok)) return;
@@ -294,14 +330,14 @@ __global__ void __launch_bounds__(ENS_BS) k_ens_stage(const __grid_constant__ En
     for_tiles<true>(A, EK_QM, [&](int, const EnsInst& I, const Consts& K, long long base, int per) {
       for (int k = threadIdx.x; k < per; k += ENS_BS) {
         const long long item = base + k;
-        if (item < K.plane) qmodes_item(K, I.UI, I.QM, item);
+        if (item < K.plane) call_qmodes(K, I.UI, I.QM, item);
       }
     });
     if (!ens_barrier(A, &s_ok)) return;
   }
-  if (!LEARNED) phase_limit<LIM_PLAIN>(A, stage == 0 ? 1 : stage, sm);
-  else if (stage <= 1) phase_limit<LIM_INFER>(A, stage == 0 ? 1 : stage, sm);
-  else phase_limit<LIM_PNET>(A, stage, sm);
+  if (!LEARNED) phase_limit<LIM_PLAIN>(A, stage == 0 ? 1 : stage);
+  else if (stage <= 1) phase_limit<LIM_INFER>(A, stage == 0 ? 1 : stage);
+  else phase_limit<LIM_PNET>(A, stage);
   if (!ens_barrier(A, &s_ok)) return;
   if (A.any_faceb && !phase_faceb(A, &s_ok)) return;
   // RK3.f90:97 / :123 set_bc after stages 1 and 2; after stage 3 (and the
@@ -589,6 +625,7 @@ int gdf_ens_create(const GdfConfig* cfgs, int32_t n, GdfEnsemble** out) {
     InstBufs& b = e->in[i];
     b.cfg = cfgs[i];
     consts_for(cfgs[i], b.K);
+    if (i == 0) ok = ok && upload_basis_once(b.K) == cudaSuccess;
     if (b.K.faceb) e->any_faceb = 1;
     const Consts& K = b.K;
     const GdfConfig& c = cfgs[i];

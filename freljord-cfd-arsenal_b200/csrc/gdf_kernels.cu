@@ -451,6 +451,27 @@ static int check_config(const GdfConfig* c) {
 
 namespace gdf {
 void consts_for(const GdfConfig& c, Consts& K) { build_consts(c, K); }
+void basis_of(const Consts& K, Basis& B) {
+  std::memcpy(B.w, K.w, sizeof(B.w));
+  std::memcpy(B.lam, K.lam, sizeof(B.lam));
+  std::memcpy(B.phiG, K.phiG, sizeof(B.phiG));
+  std::memcpy(B.phiGLL, K.phiGLL, sizeof(B.phiGLL));
+  std::memcpy(B.ppM, K.ppM, sizeof(B.ppM));
+  std::memcpy(B.phiGR, K.phiGR, sizeof(B.phiGR));
+  std::memcpy(B.phiGL, K.phiGL, sizeof(B.phiGL));
+  std::memcpy(B.phiGU, K.phiGU, sizeof(B.phiGU));
+  std::memcpy(B.phiGD, K.phiGD, sizeof(B.phiGD));
+  std::memcpy(B.phiRU, K.phiRU, sizeof(B.phiRU));
+  std::memcpy(B.phiLU, K.phiLU, sizeof(B.phiLU));
+  std::memcpy(B.phiRD, K.phiRD, sizeof(B.phiRD));
+  std::memcpy(B.phiLD, K.phiLD, sizeof(B.phiLD));
+  std::memcpy(B.mm, K.mm, sizeof(B.mm));
+  std::memcpy(B.mmE, K.mmE, sizeof(B.mmE));
+  std::memcpy(B.EzR, K.EzR, sizeof(B.EzR));
+  std::memcpy(B.EzL, K.EzL, sizeof(B.EzL));
+  std::memcpy(B.EzU, K.EzU, sizeof(B.EzU));
+  std::memcpy(B.EzD, K.EzD, sizeof(B.EzD));
+}
 int config_error(const GdfConfig* c, std::string& msg) {
   const int rc = check_config(c);
   if (rc) msg = g_err;
@@ -654,6 +675,11 @@ int gdf_create(const GdfConfig* cfg, GdfHandle** out) {
   GdfHandle* h = new GdfHandle();
   h->cfg = *cfg;
   build_consts(*cfg, h->K);
+  if (upload_basis_once(h->K) != cudaSuccess) {
+    cudaGetLastError();
+    delete h;
+    return fail(GDF_ERR_CUDA, "uploading the basis tables failed");
+  }
   const GdfConfig& c = *cfg;
   const size_t ub = uh_bytes(c), bxb = bx_bytes(c), byb = by_bytes(c);
   const size_t fxb = (size_t)h->K.fxplane * NG * NE * sizeof(double);
@@ -864,6 +890,8 @@ int gdf_lh_noalloc(const GdfConfig* cfg, const double* d_uh, double* d_du, void*
   }
   Consts K;
   build_consts(*cfg, K);
+  cudaError_t eb = upload_basis_once(K);   // first call on a device only
+  if (eb != cudaSuccess) return fail(GDF_ERR_CUDA, std::string("basis tables: ") + cudaGetErrorString(eb));
   double* Fxh = static_cast<double*>(base);
   double* Fyh = Fxh + fx * NG * NE;
   double* ezx = Fyh + fy * NG * NE;

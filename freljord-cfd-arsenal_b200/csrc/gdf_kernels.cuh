@@ -49,6 +49,21 @@ struct Consts {
   double EzxG[NG][3], EzyG[NG][3], mmE[3], EzR[3], EzL[3], EzU[3], EzD[3];
 };
 
+// The grid-independent basis tables (get_GLP.f90, get_basis.f90 on the
+// reference element): the same for every configuration, so the device holds
+// one copy (gdf_device.cuh c_basis) that every kernel reads from constant
+// memory. Consts keeps its own copy for the host.
+struct Basis {
+  double w[NG], lam[NG];
+  double phiG[NG][NG][NP];
+  double phiGLL[2][NG][NG][NP];
+  double ppM[NP];
+  double phiGR[NG][NP], phiGL[NG][NP], phiGU[NG][NP], phiGD[NG][NP];
+  double phiRU[NP], phiLU[NP], phiRD[NP], phiLD[NP];
+  double mm[NP];
+  double mmE[3], EzR[3], EzL[3], EzU[3], EzD[3];
+};
+
 // Device-resident time state of a handle (RK3.f90 t, dt).
 struct Scal {
   double t, dt, tend;
@@ -63,6 +78,7 @@ struct Scal {
 // (gdf_kernels.cu): the constants of a configuration, and the checks of a
 // configuration and of an uploaded state (0 or a GDF_ERR_* code with msg).
 void consts_for(const GdfConfig& c, Consts& K);
+void basis_of(const Consts& K, Basis& B);
 int config_error(const GdfConfig* c, std::string& msg);
 int dead_slot_error(const GdfConfig& c, const double* uh, std::string& msg);
 

@@ -427,8 +427,10 @@ class Ensemble:
 def ensemble_configs(n: int = 64, seed: int = 0, detector: int = DETECT_LEARNED):
     """The ensemble workload: instance s takes, from a generator seeded by
     (seed, s), a problem in {Orszag-Tang, rotor, blast} and a square grid side
-    in {64, 96, ..., 512}; all HLLD, the given detector (KXRCF fallback when
-    learned). Returns [(config, problem, init params or None, tend)]."""
+    in {64, 96, ..., 512}; all HLLD with the face-B minmod of the DF variants
+    (without it the rotor at 288^2 loses positivity at step 6, the reference
+    method's behaviour), the given detector (KXRCF fallback when learned).
+    Returns [(config, problem, init params or None, tend)]."""
     out = []
     for s in range(n):
         rng = np.random.default_rng([seed, s])
@@ -436,6 +438,7 @@ def ensemble_configs(n: int = 64, seed: int = 0, detector: int = DETECT_LEARNED)
         side = 64 + 32 * int(rng.integers(15))
         cfg, tend = problem_config(prob, side, side)
         cfg.flux_type = FLUX_HLLD
+        cfg.faceb_limiter = 1     # face-B minmod on every instance (see the blast and rotor notes)
         cfg.detector = detector
         if detector != DETECT_ALL:
             cfg.kxrcf_ck = 1.0
