@@ -345,6 +345,146 @@ __global__ void __launch_bounds__(ENS_BS) k_ens_stage(const __grid_constant__ En
   phase_bc(A, EK_BC, (stage == 3 || stage == 0) ? 1 : 0);
 }
 
+// ---------------------------------------------------------------------
+// Per-phase mode: the same phases as batched launches over all instances,
+// one kernel per phase, each with its own register allocation (the item
+// bodies inlined as in the single-problem kernels) and the hardware block
+// scheduler balancing the tiles; graph-captured like the persistent mode.
+__global__ void __launch_bounds__(ENS_BS) k_ep_copy(const __grid_constant__ EnsArgs A) {
+  for_tiles<true>(A, EK_COPY, [&](int, const EnsInst& I, const Consts& K, long long base, int per) {
+    const long long n = K.plane * NLIVE;
+    for (int k = threadIdx.x; k < per; k += ENS_BS) {
+      const long long item = base + k;
+      if (item >= n) break;
+      const int s = (int)(item / K.plane);
+      const long long c = (item - (long long)s * K.plane) + K.plane * (c_live_d[s] + 10 * c_live_n[s]);
+      I.UI[c] = I.U[c];
+    }
+  });
+}
+
+__global__ void __launch_bounds__(ENS_BS) k_ep_dt(const __grid_constant__ EnsArgs A) {
+  __shared__ double s_x[ENS_BS], s_y[ENS_BS];
+  for_tiles<false>(A, EK_DT, [&](int i, const EnsInst& I, const Consts& K, long long base, int per) {
+    const long long n = (long long)K.nx * K.ny;
+    double ax = 0.0, ay = 0.0;
+    for (int k = threadIdx.x; k < per; k += ENS_BS) {
+      const long long item = base + k;
+      if (item < n) dt_cell_speeds(K, I.U, item, ax, ay, I.sc);
+    }
+    __syncthreads();
+    s_x[threadIdx.x] = ax;
+    s_y[threadIdx.x] = ay;
+    __syncthreads();
+    for (int s = ENS_BS / 2; s > 0; s >>= 1) {
+      if (threadIdx.x < s) {
+        s_x[threadIdx.x] = max_ign_nan(s_x[threadIdx.x], s_x[threadIdx.x + s]);
+        s_y[threadIdx.x] = max_ign_nan(s_y[threadIdx.x], s_y[threadIdx.x + s]);
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      atomicMax(&A.amax[2 * i], (unsigned long long)__double_as_longlong(s_x[0]));
+      atomicMax(&A.amax[2 * i + 1], (unsigned long long)__double_as_longlong(s_y[0]));
+    }
+  });
+}
+
+__global__ void k_ep_dt_final(const __grid_constant__ EnsArgs A) {
+  for (int i = threadIdx.x; i < A.n; i += blockDim.x) {
+    const EnsInst& I = A.inst[i];
+    const double ax = __longlong_as_double((long long)A.amax[2 * i]);
+    const double ay = __longlong_as_double((long long)A.amax[2 * i + 1]);
+    A.amax[2 * i] = 0ull;
+    A.amax[2 * i + 1] = 0ull;
+    dt_advance(*I.K, ax, ay, I.sc, 1);
+  }
+}
+
+__global__ void __launch_bounds__(ENS_BS) k_ep_bc(const __grid_constant__ EnsArgs A, int kind, int zeroB) {
+  phase_bc(A, kind, zeroB);
+}
+
+__global__ void __launch_bounds__(ENS_BS) k_ep_faces(const __grid_constant__ EnsArgs A) {
+  for_tiles<true>(A, EK_FX, [&](int, const EnsInst& I, const Consts& K, long long base, int per) {
+    const long long n = face_items<0>(K);
+    for (int k = threadIdx.x; k < per; k += ENS_BS) {
+      const long long item = base + k;
+      if (item < n) face_item<0>(K, I.U, I.Fxh, I.EzRL, item);
+    }
+  });
+  for_tiles<true>(A, EK_FY, [&](int, const EnsInst& I, const Consts& K, long long base, int per) {
+    const long long n = face_items<1>(K);
+    for (int k = threadIdx.x; k < per; k += ENS_BS) {
+      const long long item = base + k;
+      if (item < n) face_item<1>(K, I.U, I.Fyh, I.EzUD, item);
+    }
+  });
+  for_tiles<true>(A, EK_VX, [&](int, const EnsInst& I, const Consts& K, long long base, int per) {
+    for (int k = threadIdx.x; k < per; k += ENS_BS) {
+      const long long item = base + k;
+      if (item < K.vplane) vertex_item(K, I.U, I.EzV, item);
+    }
+  });
+}
+
+__global__ void __launch_bounds__(ENS_BS) k_ep_cell(const __grid_constant__ EnsArgs A, int stage) {
+  __shared__ double ms[NLIVE * ENS_BS];
+  for_tiles<true>(A, EK_CELL, [&](int, const EnsInst& I, const Consts& K, long long base, int per) {
+    for (int k = threadIdx.x; k < per; k += ENS_BS) {
+      const long long item = base + k;
+      if (item < K.plane) cell_item(K, I.U, I.U0, I.UI, I.Fxh, I.Fyh, nullptr, I.sc, stage, item, ms);
+    }
+  });
+}
+
+__global__ void __launch_bounds__(ENS_BS) k_ep_bface(const __grid_constant__ EnsArgs A, int stage) {
+  for_tiles<true>(A, EK_BF, [&](int, const EnsInst& I, const Consts& K, long long base, int per) {
+    const long long n = K.fxplane + K.fyplane;
+    for (int k = threadIdx.x; k < per; k += ENS_BS) {
+      const long long item = base + k;
+      if (item < n)
+        bface_item(K, I.EzRL, I.EzUD, I.EzV, I.BX, I.BX0, I.BXI, I.BY, I.BY0, I.BYI, nullptr, nullptr, I.sc, stage,
+                   item);
+    }
+  });
+}
+
+__global__ void __launch_bounds__(ENS_BS) k_ep_qmodes(const __grid_constant__ EnsArgs A) {
+  for_tiles<true>(A, EK_QM, [&](int, const EnsInst& I, const Consts& K, long long base, int per) {
+    for (int k = threadIdx.x; k < per; k += ENS_BS) {
+      const long long item = base + k;
+      if (item < K.plane) qmodes_item(K, I.UI, I.QM, item);
+    }
+  });
+}
+
+template <int LM>
+__global__ void __launch_bounds__(ENS_BS) k_ep_limit(const __grid_constant__ EnsArgs A, int stage) {
+  extern __shared__ __align__(16) unsigned char lsm[];
+  for_tiles<true>(A, EK_LIM, [&](int, const EnsInst& I, const Consts& K, long long base, int) {
+    limit_item<LM>(K, I.UI, I.U, I.BX, I.BY, I.flags, I.trouble, stage, K.faceb ? 0 : 1, I.sc, A.net, I.QM, I.pnet,
+                   A.t_lo, A.t_hi, base + threadIdx.x, lsm);
+    if (LM == LIM_INFER) __syncthreads();
+  });
+}
+
+__global__ void __launch_bounds__(ENS_BS) k_ep_faceb(const __grid_constant__ EnsArgs A) {
+  for_tiles<true>(A, EK_FB, [&](int, const EnsInst& I, const Consts& K, long long base, int per) {
+    for (int k = threadIdx.x; k < per; k += ENS_BS) faceb_item(K, I.U, I.BX, I.BY, base + k);
+  });
+}
+
+__global__ void __launch_bounds__(ENS_BS) k_ep_divfree(const __grid_constant__ EnsArgs A) {
+  for_tiles<true>(A, EK_DF, [&](int, const EnsInst& I, const Consts& K, long long base, int per) {
+    const long long n = (long long)K.nx * K.ny;
+    for (int k = threadIdx.x; k < per; k += ENS_BS) {
+      const long long item = base + k;
+      if (item < n) divfree_item(K, I.U, I.BX, I.BY, item);
+    }
+  });
+}
+
 thread_local std::string g_ens_err;
 int efail(int code, const std::string& m) {
   g_ens_err = m;
@@ -392,11 +532,13 @@ struct GdfEnsemble {
   int cell_per_thread = 1;     // cells per thread of the residual tiles
   int grid = 0;
   int sms = 0;
+  int mode = 0;                // 0: one persistent kernel per stage; 1: one launch per phase
   EnsArgs args{};
   cudaGraphExec_t graph = nullptr;
   int graph_ok = 1;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int64_t launches = 0;
+  int64_t step_launches = 3;
 };
 
 namespace {
@@ -455,6 +597,8 @@ int ens_layout(GdfEnsemble* e) {
   int occ = 0;
   const size_t smem = ens_smem(e->learned);
   ECK(cudaFuncSetAttribute(stage_kernel(e->learned), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  ECK(cudaFuncSetAttribute(k_ep_limit<LIM_INFER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)LIMIT_SMEM_LEARNED));
   ECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, stage_kernel(e->learned), ENS_BS, smem));
   if (occ < 1) return efail(GDF_ERR_CUDA, "the ensemble stage kernel cannot be resident");
   const int per_sm = e->ctas_per_sm > 0 ? std::min(e->ctas_per_sm, occ) : occ;
@@ -476,7 +620,7 @@ int ens_layout(GdfEnsemble* e) {
   return GDF_OK;
 }
 
-int launch_stage_ens(GdfEnsemble* e, int stage) {
+int launch_stage_persistent(GdfEnsemble* e, int stage) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)e->grid);
   cfg.blockDim = dim3(ENS_BS);
@@ -492,6 +636,63 @@ int launch_stage_ens(GdfEnsemble* e, int stage) {
   e->launches++;
   if (err != cudaSuccess) return efail(GDF_ERR_CUDA, std::string("ensemble stage launch: ") + cudaGetErrorString(err));
   return GDF_OK;
+}
+
+// grid of a phase launch: one block per tile (at least one block)
+unsigned tiles_of(const EnsArgs& A, int kind) { return (unsigned)std::max(A.total[kind], 1); }
+
+int launch_stage_phases(GdfEnsemble* e, int stage) {
+  const EnsArgs& A = e->args;
+  cudaStream_t st = e->st;
+  int n = 0;
+  auto bc = [&](int kind, int zeroB) {
+    k_ep_bc<<<tiles_of(A, kind), ENS_BS, 0, st>>>(A, kind, zeroB);
+    ++n;
+  };
+  if (stage == 0) {
+    bc(EK_BC, 0);
+    k_ep_copy<<<tiles_of(A, EK_COPY), ENS_BS, 0, st>>>(A);
+    ++n;
+  } else {
+    if (stage == 1) {
+      k_ep_dt<<<tiles_of(A, EK_DT), ENS_BS, 0, st>>>(A);
+      k_ep_dt_final<<<1, 128, 0, st>>>(A);
+      n += 2;
+      bc(EK_BC, 0);
+    }
+    const unsigned gf = std::max(tiles_of(A, EK_FX), std::max(tiles_of(A, EK_FY), tiles_of(A, EK_VX)));
+    k_ep_faces<<<gf, ENS_BS, 0, st>>>(A);
+    k_ep_cell<<<tiles_of(A, EK_CELL), ENS_BS, 0, st>>>(A, stage);
+    k_ep_bface<<<tiles_of(A, EK_BF), ENS_BS, 0, st>>>(A, stage);
+    n += 3;
+  }
+  const int ls = stage == 0 ? 1 : stage;
+  if (e->learned && stage <= 1) {
+    k_ep_qmodes<<<tiles_of(A, EK_QM), ENS_BS, 0, st>>>(A);
+    k_ep_limit<LIM_INFER><<<tiles_of(A, EK_LIM), ENS_BS, LIMIT_SMEM_LEARNED, st>>>(A, ls);
+    n += 2;
+  } else if (e->learned) {
+    k_ep_limit<LIM_PNET><<<tiles_of(A, EK_LIM), ENS_BS, 0, st>>>(A, ls);
+    ++n;
+  } else {
+    k_ep_limit<LIM_PLAIN><<<tiles_of(A, EK_LIM), ENS_BS, 0, st>>>(A, ls);
+    ++n;
+  }
+  if (A.any_faceb) {
+    bc(EK_BCF, 0);
+    k_ep_faceb<<<tiles_of(A, EK_FB), ENS_BS, 0, st>>>(A);
+    k_ep_divfree<<<tiles_of(A, EK_DF), ENS_BS, 0, st>>>(A);
+    n += 2;
+  }
+  bc(EK_BC, (stage == 3 || stage == 0) ? 1 : 0);
+  e->launches += n;
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return efail(GDF_ERR_CUDA, std::string("ensemble phase launch: ") + cudaGetErrorString(err));
+  return GDF_OK;
+}
+
+int launch_stage_ens(GdfEnsemble* e, int stage) {
+  return e->mode == 1 ? launch_stage_phases(e, stage) : launch_stage_persistent(e, stage);
 }
 
 int launch_step_ens(GdfEnsemble* e) {
@@ -514,6 +715,7 @@ int ensure_graph_ens(GdfEnsemble* e) {
   }
   const int64_t l0 = e->launches;
   int rc = launch_step_ens(e);
+  e->step_launches = e->launches - l0;
   e->launches = l0;
   cudaError_t ce = cudaStreamEndCapture(e->st, &g);
   if (rc || ce != cudaSuccess || !g) {
@@ -538,7 +740,7 @@ int run_steps(GdfEnsemble* e, int steps) {
   for (int k = 0; k < steps; ++k) {
     if (e->graph) {
       ECK(cudaGraphLaunch(e->graph, e->st));
-      e->launches += 3;
+      e->launches += e->step_launches;
     } else if ((rc = launch_step_ens(e))) {
       return rc;
     }
@@ -798,9 +1000,20 @@ int gdf_ens_set_tiles(GdfEnsemble* e, int32_t ctas_per_sm, int32_t face_per_thre
   return ens_layout(e);
 }
 
+int gdf_ens_set_mode(GdfEnsemble* e, int32_t mode) {
+  if (!e || (mode != 0 && mode != 1)) return efail(GDF_ERR_ARG, "mode must be 0 (persistent) or 1 (per phase)");
+  e->mode = mode;
+  if (e->graph) {
+    cudaGraphExecDestroy(e->graph);
+    e->graph = nullptr;
+  }
+  return GDF_OK;
+}
+
 int gdf_ens_get_tiles(GdfEnsemble* e, int32_t* ctas_per_sm, int32_t* face_per_thread, int32_t* cell_per_thread,
-                      int32_t* grid, int32_t* graph) {
+                      int32_t* grid, int32_t* graph, int32_t* mode) {
   if (!e) return efail(GDF_ERR_ARG, "null handle");
+  if (mode) *mode = e->mode;
   if (ctas_per_sm) *ctas_per_sm = e->grid / std::max(e->sms, 1);
   if (face_per_thread) *face_per_thread = e->face_per_thread;
   if (cell_per_thread) *cell_per_thread = e->cell_per_thread;
@@ -809,10 +1022,13 @@ int gdf_ens_get_tiles(GdfEnsemble* e, int32_t* ctas_per_sm, int32_t* face_per_th
   return GDF_OK;
 }
 
-// Times `steps` steps for every tile shape of the candidate set from the
-// same state (saved before, restored after each trial, so the ensemble's
-// trajectory is unchanged) and keeps the fastest. ms_out[k] (optional, 36
-// entries) receives the candidates' ms per step, -1 where not resident.
+// Times `steps` steps for every candidate (execution mode x tile shape)
+// from the same state (saved before, restored after each trial, so the
+// ensemble's trajectory is unchanged) and keeps the fastest. ms_out
+// (optional, GDF_ENS_TUNE_CANDIDATES entries) receives the candidates' ms per
+// step, -1 where not resident: first the persistent mode (blocks per SM 1..4
+// x face items 1, 2, 4 x cells 1, 2, 4), then the per-phase mode (face items
+// x cells).
 int gdf_ens_tune(GdfEnsemble* e, int32_t steps, float* ms_out) {
   int rc = ens_ready(e);
   if (rc) return rc;
@@ -847,32 +1063,35 @@ int gdf_ens_tune(GdfEnsemble* e, int32_t steps, float* ms_out) {
   ECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, stage_kernel(e->learned), ENS_BS, ens_smem(e->learned)));
   const int faces[3] = {1, 2, 4}, cells[3] = {1, 2, 4};
   float best = 1e30f;
-  int bc = 0, bf = 1, bcell = 1, k = 0;
-  for (int cps = 1; cps <= 4; ++cps)
-    for (int fi = 0; fi < 3; ++fi)
-      for (int ci = 0; ci < 3; ++ci, ++k) {
-        if (cps > occ) {
-          if (ms_out) ms_out[k] = -1.f;
-          continue;
+  int bmode = 0, bc = 0, bf = 1, bcell = 1, k = 0;
+  for (int mode = 0; mode <= 1; ++mode)
+    for (int cps = 1; cps <= (mode == 0 ? 4 : 1); ++cps)
+      for (int fi = 0; fi < 3; ++fi)
+        for (int ci = 0; ci < 3; ++ci, ++k) {
+          if (mode == 0 && cps > occ) {
+            if (ms_out) ms_out[k] = -1.f;
+            continue;
+          }
+          if ((rc = gdf_ens_set_mode(e, mode))) return rc;
+          if ((rc = gdf_ens_set_tiles(e, mode == 0 ? cps : 0, faces[fi], cells[ci]))) return rc;
+          if ((rc = run_steps(e, 1))) return rc;   // warm-up (and graph capture)
+          if ((rc = copy_state(false))) return rc;
+          ECK(cudaEventRecord(e->ev0, e->st));
+          if ((rc = run_steps(e, steps))) return rc;
+          ECK(cudaEventRecord(e->ev1, e->st));
+          ECK(cudaEventSynchronize(e->ev1));
+          float ms = 0.f;
+          ECK(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
+          ms /= (float)steps;
+          if (ms_out) ms_out[k] = ms;
+          if ((rc = check_health(e))) return rc;
+          if ((rc = copy_state(false))) return rc;
+          if (ms < best) {
+            best = ms;
+            bmode = mode; bc = mode == 0 ? cps : 0; bf = faces[fi]; bcell = cells[ci];
+          }
         }
-        if ((rc = gdf_ens_set_tiles(e, cps, faces[fi], cells[ci]))) return rc;
-        if ((rc = run_steps(e, 1))) return rc;   // warm-up (and graph capture)
-        if ((rc = copy_state(false))) return rc;
-        ECK(cudaEventRecord(e->ev0, e->st));
-        if ((rc = run_steps(e, steps))) return rc;
-        ECK(cudaEventRecord(e->ev1, e->st));
-        ECK(cudaEventSynchronize(e->ev1));
-        float ms = 0.f;
-        ECK(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
-        ms /= (float)steps;
-        if (ms_out) ms_out[k] = ms;
-        if ((rc = check_health(e))) return rc;
-        if ((rc = copy_state(false))) return rc;
-        if (ms < best) {
-          best = ms;
-          bc = cps; bf = faces[fi]; bcell = cells[ci];
-        }
-      }
+  if ((rc = gdf_ens_set_mode(e, bmode))) return rc;
   if ((rc = gdf_ens_set_tiles(e, bc, bf, bcell))) return rc;
   ECK(cudaStreamSynchronize(e->st));
   return GDF_OK;

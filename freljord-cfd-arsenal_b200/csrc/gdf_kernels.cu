@@ -36,6 +36,15 @@
 #ifndef GDF_EXACT
 #define GDF_EXACT 0
 #endif
+// minimum resident blocks per SM requested of the face/vertex (128-thread)
+// and residual (64-thread) kernels: the register budget per thread they
+// allow (65536 / (threads x blocks)); arithmetic is the same for any value
+#ifndef GDF_FACE_MINB
+#define GDF_FACE_MINB 1
+#endif
+#ifndef GDF_CELL_MINB
+#define GDF_CELL_MINB 1
+#endif
 
 
 namespace gdf {
@@ -52,7 +61,7 @@ __global__ void k_set_bc(const __grid_constant__ Consts K, double* __restrict__ 
 }
 
 template <int DIR>
-__global__ void __launch_bounds__(128) k_face(const __grid_constant__ Consts K, const double* __restrict__ U,
+__global__ void __launch_bounds__(128, GDF_FACE_MINB) k_face(const __grid_constant__ Consts K, const double* __restrict__ U,
                                               double* __restrict__ Fh_out, double* __restrict__ Ez_out,
                                               const Scal* __restrict__ sc) {
   if (sc && !sc->active) return;
@@ -61,7 +70,7 @@ __global__ void __launch_bounds__(128) k_face(const __grid_constant__ Consts K, 
   face_item<DIR>(K, U, Fh_out, Ez_out, item);
 }
 
-__global__ void __launch_bounds__(128) k_vertex(const __grid_constant__ Consts K, const double* __restrict__ U,
+__global__ void __launch_bounds__(128, GDF_FACE_MINB) k_vertex(const __grid_constant__ Consts K, const double* __restrict__ U,
                                                 double* __restrict__ EzV, const Scal* __restrict__ sc) {
   if (sc && !sc->active) return;
   const long long item = gtid();
@@ -69,7 +78,7 @@ __global__ void __launch_bounds__(128) k_vertex(const __grid_constant__ Consts K
   vertex_item(K, U, EzV, item);
 }
 
-__global__ void __launch_bounds__(CELL_BS) k_cell(const __grid_constant__ Consts K, const double* __restrict__ U,
+__global__ void __launch_bounds__(CELL_BS, GDF_CELL_MINB) k_cell(const __grid_constant__ Consts K, const double* __restrict__ U,
                                                   double* __restrict__ U0, double* __restrict__ UI,
                                                   const double* __restrict__ Fxh, const double* __restrict__ Fyh,
                                                   double* __restrict__ duout, const Scal* __restrict__ sc, int stage) {

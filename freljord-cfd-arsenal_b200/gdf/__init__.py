@@ -29,6 +29,7 @@ from ._abi import (BC_OUTFLOW, BC_PERIODIC, DETECT_ALL, DETECT_KXRCF, FLUX_HLL, 
                    problem_config, reference_config, uh_shape)
 
 DETECT_LEARNED = 2
+ENS_TUNE_CANDIDATES = 45
 MLP_NPARAM = 10049
 NFEAT = 90
 
@@ -108,7 +109,8 @@ def load(exact: bool = True):
     L.gdf_ens_prepare.argtypes = [vp]
     L.gdf_ens_advance.argtypes = [vp, i32, C.POINTER(C.c_int64), C.POINTER(i32), C.POINTER(C.c_double)]
     L.gdf_ens_set_tiles.argtypes = [vp, i32, i32, i32]
-    L.gdf_ens_get_tiles.argtypes = [vp] + [C.POINTER(i32)] * 5
+    L.gdf_ens_get_tiles.argtypes = [vp] + [C.POINTER(i32)] * 6
+    L.gdf_ens_set_mode.argtypes = [vp, i32]
     L.gdf_ens_tune.argtypes = [vp, i32, C.POINTER(C.c_float)]
     L.gdf_ens_kernel_launches.argtypes = [vp]
     L.gdf_ens_kernel_launches.restype = C.c_int64
@@ -410,13 +412,18 @@ class Ensemble:
     def set_tiles(self, ctas_per_sm: int = 0, face_per_thread: int = 1, cell_per_thread: int = 1) -> None:
         self._ck(self.L.gdf_ens_set_tiles(self.h, ctas_per_sm, face_per_thread, cell_per_thread))
 
+    def set_mode(self, mode: int) -> None:
+        """0: one persistent kernel per RK stage; 1: one launch per phase."""
+        self._ck(self.L.gdf_ens_set_mode(self.h, mode))
+
     def tiles(self) -> dict:
-        v = [C.c_int32() for _ in range(5)]
+        v = [C.c_int32() for _ in range(6)]
         self._ck(self.L.gdf_ens_get_tiles(self.h, *[C.byref(x) for x in v]))
-        return dict(zip(["ctas_per_sm", "face_per_thread", "cell_per_thread", "grid", "graph"], [x.value for x in v]))
+        return dict(zip(["ctas_per_sm", "face_per_thread", "cell_per_thread", "grid", "graph", "mode"],
+                        [x.value for x in v]))
 
     def tune(self, steps: int = 2):
-        ms = np.zeros(36, np.float32)
+        ms = np.zeros(ENS_TUNE_CANDIDATES, np.float32)
         self._ck(self.L.gdf_ens_tune(self.h, steps, _fptr(ms)))
         return ms
 

@@ -240,12 +240,19 @@ int gdf_ens_advance(GdfEnsemble *e, int32_t steps, int64_t *cell_updates, int32_
  * many faces), cells per thread of the residual tiles (a block 64x). */
 int gdf_ens_set_tiles(GdfEnsemble *e, int32_t ctas_per_sm, int32_t face_per_thread,
                       int32_t cell_per_thread);
+/* Execution mode: 0 = one persistent cooperative kernel per RK stage (grid
+ * barriers between phases); 1 = one batched launch per phase over all
+ * instances. Both are graph-captured and give identical results. */
+int gdf_ens_set_mode(GdfEnsemble *e, int32_t mode);
 int gdf_ens_get_tiles(GdfEnsemble *e, int32_t *ctas_per_sm, int32_t *face_per_thread,
-                      int32_t *cell_per_thread, int32_t *grid, int32_t *graph);
-/* Autotuner: times `steps` steps of each of the 36 candidate tile shapes
- * (blocks per SM 1..4 x face items 1,2,4 x cells 1,2,4) from the current
- * state, restoring the state after every trial, and keeps the fastest.
- * ms_out (36 floats, or NULL) receives ms per step, -1 where not resident. */
+                      int32_t *cell_per_thread, int32_t *grid, int32_t *graph, int32_t *mode);
+/* Autotuner: times `steps` steps of each candidate from the current state,
+ * restoring the state after every trial, and keeps the fastest: the
+ * persistent mode with blocks per SM 1..4 x face items 1,2,4 x cells
+ * 1,2,4 (36), then the per-phase mode with face items x cells (9). ms_out
+ * (GDF_ENS_TUNE_CANDIDATES floats, or NULL) receives ms per step, -1 where
+ * not resident. */
+enum { GDF_ENS_TUNE_CANDIDATES = 45 };
 int gdf_ens_tune(GdfEnsemble *e, int32_t steps, float *ms_out);
 int64_t gdf_ens_kernel_launches(GdfEnsemble *e);
 const char *gdf_ens_last_error(void);

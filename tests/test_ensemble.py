@@ -57,12 +57,14 @@ def same(a, b):
     return all(np.array_equal(x, y) for x, y in zip(a, b))
 
 
-def test_ensemble_matches_single_problem_handles():
+@pytest.mark.parametrize("mode", [0, 1], ids=["persistent", "per-phase"])
+def test_ensemble_matches_single_problem_handles(mode):
     insts = mixed_instances()
     # the vortex instance stops after about two steps: its end time is short
     tends = [1e9] * len(insts)
     tends[4] = 0.07
     e = make_ensemble(insts, tends=tends)
+    e.set_mode(mode)
     steps = 5
     cu, active, ms = e.advance(steps)
     assert ms > 0
@@ -78,11 +80,12 @@ def test_ensemble_matches_single_problem_handles():
     assert cu == total and active == len(insts) - 1
 
 
-def test_tile_shapes_give_identical_results():
+def test_tile_shapes_and_modes_give_identical_results():
     insts = mixed_instances()[:3]
     res = []
-    for tiles in [(0, 1, 1), (1, 4, 2), (2, 2, 4)]:
+    for mode, tiles in [(0, (0, 1, 1)), (0, (1, 4, 2)), (0, (2, 2, 4)), (1, (0, 1, 1)), (1, (0, 4, 2))]:
         e = make_ensemble(insts)
+        e.set_mode(mode)
         e.set_tiles(*tiles)
         e.advance(3)
         res.append([e.download(i) for i in range(len(insts))])
@@ -95,9 +98,9 @@ def test_autotuner_keeps_the_trajectory():
     insts = mixed_instances()[:4]
     a = make_ensemble(insts)
     ms = a.tune(1)
-    assert ms.shape == (36,) and (ms > 0).any()
+    assert ms.shape == (gdf.ENS_TUNE_CANDIDATES,) and (ms[:36] > 0).any() and (ms[36:] > 0).all()
     tl = a.tiles()
-    assert tl["grid"] > 0 and tl["face_per_thread"] in (1, 2, 4)
+    assert tl["grid"] > 0 and tl["face_per_thread"] in (1, 2, 4) and tl["mode"] in (0, 1)
     a.advance(3)
     b = make_ensemble(insts)
     b.advance(3)
@@ -106,7 +109,8 @@ def test_autotuner_keeps_the_trajectory():
         assert a.time(i) == b.time(i)
 
 
-def test_learned_ensemble_matches_single_problem_handles():
+@pytest.mark.parametrize("mode", [0, 1], ids=["persistent", "per-phase"])
+def test_learned_ensemble_matches_single_problem_handles(mode):
     net = gdf.Mlp(11)
     insts = []
     for cfg, prob, params, tend in mixed_instances()[:4]:
@@ -115,6 +119,7 @@ def test_learned_ensemble_matches_single_problem_handles():
         insts.append((cfg, prob, params, tend))
     lohi = (0.3, 0.7)
     e = make_ensemble(insts, net, lohi)
+    e.set_mode(mode)
     e.advance(3)
     for i, (cfg, prob, params, tend) in enumerate(insts):
         ref, t_ref = run_single(cfg, prob, params, tend, 3, net, lohi)
@@ -138,6 +143,8 @@ def test_ensemble_errors():
         e.set_indicator(gdf.Mlp(0))         # detectors are not learned
     with pytest.raises(gdf.GdfError):
         e.set_tiles(0, 0, 1)
+    with pytest.raises(gdf.GdfError):
+        e.set_mode(2)
     cfg = insts[0][0].copy()
     cfg.nx = 1
     with pytest.raises(gdf.GdfError):
