@@ -405,7 +405,7 @@ __global__ void __launch_bounds__(ENS_BS) k_ep_bc(const __grid_constant__ EnsArg
   phase_bc(A, kind, zeroB);
 }
 
-__global__ void __launch_bounds__(ENS_BS) k_ep_faces(const __grid_constant__ EnsArgs A) {
+__global__ void __launch_bounds__(ENS_BS, 8) k_ep_faces(const __grid_constant__ EnsArgs A) {
   for_tiles<true>(A, EK_FX, [&](int, const EnsInst& I, const Consts& K, long long base, int per) {
     const long long n = face_items<0>(K);
     for (int k = threadIdx.x; k < per; k += ENS_BS) {
