@@ -532,7 +532,7 @@ struct GdfEnsemble {
   int cell_per_thread = 1;     // cells per thread of the residual tiles
   int grid = 0;
   int sms = 0;
-  int mode = 0;                // 0: one persistent kernel per stage; 1: one launch per phase
+  int mode = 1;                // 0: one persistent kernel per stage; 1: one launch per phase (faster here)
   EnsArgs args{};
   cudaGraphExec_t graph = nullptr;
   int graph_ok = 1;
