@@ -725,17 +725,18 @@ static __device__ void pp_cell(const Consts& K, double (*m)[NP]) {
 // LIM_PNET, the learned gate on the step's stored probabilities (stages 2
 // and 3: the network sees the step's stage-1 pre-limit state).
 constexpr int LIM_PLAIN = 0, LIM_INFER = 1, LIM_PNET = 2;
+// Limiter of one interior cell in three pieces, composed by limit_item:
+//   lim_gate    loads the pre-limit modes and decides the gate (detector,
+//               sticky KXRCF flag, learned probability); LIM_INFER runs the
+//               network for the block first (block-cooperative)
+//   lim_tvb     characteristic TVB limiting of a gated cell
+//   lim_finish  positivity limiter, div-free reconstruction, store, flags
 template <int LM>
-__device__ __forceinline__ void limit_item(const Consts& K, const double* __restrict__ S, double* __restrict__ D,
-                                           const double* __restrict__ BX, const double* __restrict__ BY,
-                                           int32_t* __restrict__ flags, int32_t* __restrict__ trouble, int stage,
-                                           int divfree, Scal* __restrict__ sc, const MlpDev* __restrict__ net,
-                                           const float* __restrict__ QM, float* __restrict__ pnet,
-                                           float t_lo, float t_hi, long long item, unsigned char* lsm) {
-  const bool valid = item < (long long)K.nx * K.ny;
-  const int i = valid ? (int)(item % K.nx) + 1 : 1;
-  const int j = valid ? (int)(item / K.nx) + 1 : 1;
-  const long long c = i + (long long)K.nx2 * j;
+__device__ __forceinline__ bool lim_gate(const Consts& K, const double* __restrict__ S, int32_t* __restrict__ trouble,
+                                         const MlpDev* __restrict__ net, const float* __restrict__ QM,
+                                         float* __restrict__ pnet, float t_lo, float t_hi, long long item,
+                                         unsigned char* lsm, bool valid, long long c, double (*m)[NP],
+                                         int32_t& word) {
   const long long pl = K.plane;
   float p_net = 0.f;
   if (LM == LIM_INFER) {
@@ -786,13 +787,12 @@ __device__ __forceinline__ void limit_item(const Consts& K, const double* __rest
   } else if (LM == LIM_PNET) {
     if (valid) p_net = pnet[item];
   }
-  if (!valid) return;
-  double m[NE][NP];
+  if (!valid) return false;
 #pragma unroll
   for (int n = 0; n < NE; ++n)
 #pragma unroll
     for (int d = 0; d < NP; ++d) m[n][d] = live_mode(n, d) ? S[c + pl * (d + 10 * n)] : 0.0;
-  int32_t word = 0;
+  word = 0;
   bool gate = true;
   if (K.detector == GDF_DETECT_KXRCF) {
     const bool prev = K.sticky ? (trouble[item] != 0) : false;
@@ -807,7 +807,12 @@ __device__ __forceinline__ void limit_item(const Consts& K, const double* __rest
     else gate = false;
     if (gate) word |= (1 << 24);
   }
-  if (gate) {
+  return gate;
+}
+
+__device__ __forceinline__ void lim_tvb(const Consts& K, const double* __restrict__ S, long long c,
+                                        double (*m)[NP], int32_t& word) {
+  const long long pl = K.plane;
     const double c23 = 2.0 / 3.0;
     const double rhoij = m[0][0];
     const double u1 = m[1][0] / rhoij, u2 = m[2][0] / rhoij, u3 = m[3][0] / rhoij;
@@ -883,6 +888,12 @@ __device__ __forceinline__ void limit_item(const Consts& K, const double* __rest
     }
     word |= (int32_t)change;
   }
+
+__device__ __forceinline__ void lim_finish(const Consts& K, double* __restrict__ D, const double* __restrict__ BX,
+                                           const double* __restrict__ BY, int32_t* __restrict__ flags, int stage,
+                                           int divfree, Scal* __restrict__ sc, long long item, int i, int j,
+                                           long long c, double (*m)[NP], int32_t word) {
+  const long long pl = K.plane;
   if (K.pp) pp_cell(K, m);
   if (divfree) {
     // div_free_Balsara.f90:30-75 from the four face polynomials
@@ -925,6 +936,25 @@ __device__ __forceinline__ void limit_item(const Consts& K, const double* __rest
     if (stage <= 1) flags[item] = w; else flags[item] |= w;
   }
   if (!(m[0][0] > 0.0) || !isfinite(m[4][0])) atomicOr(&sc->status, 1);
+}
+
+template <int LM>
+__device__ __forceinline__ void limit_item(const Consts& K, const double* __restrict__ S, double* __restrict__ D,
+                                           const double* __restrict__ BX, const double* __restrict__ BY,
+                                           int32_t* __restrict__ flags, int32_t* __restrict__ trouble, int stage,
+                                           int divfree, Scal* __restrict__ sc, const MlpDev* __restrict__ net,
+                                           const float* __restrict__ QM, float* __restrict__ pnet,
+                                           float t_lo, float t_hi, long long item, unsigned char* lsm) {
+  const bool valid = item < (long long)K.nx * K.ny;
+  const int i = valid ? (int)(item % K.nx) + 1 : 1;
+  const int j = valid ? (int)(item / K.nx) + 1 : 1;
+  const long long c = i + (long long)K.nx2 * j;
+  double m[NE][NP];
+  int32_t word = 0;
+  const bool gate = lim_gate<LM>(K, S, trouble, net, QM, pnet, t_lo, t_hi, item, lsm, valid, c, m, word);
+  if (!valid) return;
+  if (gate) lim_tvb(K, S, c, m, word);
+  lim_finish(K, D, BX, BY, flags, stage, divfree, sc, item, i, j, c, m, word);
 }
 
 // Face-B TVB limiter of TVB_Limiter_P2.f90:128-187 (applied when enabled):
