@@ -614,13 +614,35 @@ static int check_dead_slots(const GdfConfig& c, const double* uh) {
   for (int n = 0; n < NE; ++n)
     for (int d = 0; d < NP; ++d) {
       if (live_mode(n, d)) continue;
-      const double* p = uh + plane * (d + 10 * n);
-      for (size_t q = 0; q < plane; ++q)
-        if (p[q] != 0.0)
-          return fail(GDF_ERR_ARG, "uh has a nonzero value in mode " + std::to_string(d + 1) + " of variable " +
-                                       std::to_string(n + 1) + ", which the P2 scheme never populates");
+      // +0 and -0 pass, anything else (NaN included) fails: OR of the bit
+      // patterns without the sign bit, a loop the compiler vectorises
+      const uint64_t* w = reinterpret_cast<const uint64_t*>(uh + plane * (d + 10 * n));
+      uint64_t acc = 0;
+      for (size_t q = 0; q < plane; ++q) acc |= w[q] << 1;
+      if (acc != 0)
+        return fail(GDF_ERR_ARG, "uh has a nonzero value in mode " + std::to_string(d + 1) + " of variable " +
+                                     std::to_string(n + 1) + ", which the P2 scheme never populates");
     }
   return GDF_OK;
+}
+
+// Host-to-device copy of the 52 live slot planes of uh (the device copy's
+// dead slots are zero from allocation and no kernel writes them).
+static cudaError_t upload_live(double* dst, const double* uh, const GdfConfig& c, cudaStream_t st) {
+  const size_t plane = (size_t)(c.nx + 2) * (c.ny + 2);
+  for (int n = 0; n < NE; ++n) {
+    // live slots of a variable are modes 0..5 plus (Bx) 6, 8 or (By) 7, 9
+    const size_t o = plane * (10 * n);
+    cudaError_t e = cudaMemcpyAsync(dst + o, uh + o, 6 * plane * sizeof(double), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return e;
+    for (int d = 6; d < NP; ++d) {
+      if (!live_mode(n, d)) continue;
+      e = cudaMemcpyAsync(dst + o + plane * d, uh + o + plane * d, plane * sizeof(double), cudaMemcpyHostToDevice,
+                          st);
+      if (e != cudaSuccess) return e;
+    }
+  }
+  return cudaSuccess;
 }
 
 namespace gdf {
@@ -760,7 +782,7 @@ int gdf_upload(GdfHandle* h, const double* uh, const double* bx, const double* b
   if (!h || !uh || !bx || !by) return fail(GDF_ERR_ARG, "null argument");
   int rc = check_dead_slots(h->cfg, uh);
   if (rc) return rc;
-  CK(cudaMemcpyAsync(h->U, uh, uh_bytes(h->cfg), cudaMemcpyHostToDevice, h->st));
+  CK(upload_live(h->U, uh, h->cfg, h->st));
   CK(cudaMemcpyAsync(h->BX, bx, bx_bytes(h->cfg), cudaMemcpyHostToDevice, h->st));
   CK(cudaMemcpyAsync(h->BY, by, by_bytes(h->cfg), cudaMemcpyHostToDevice, h->st));
   CK(cudaStreamSynchronize(h->st));
