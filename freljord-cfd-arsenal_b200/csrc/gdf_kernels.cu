@@ -626,19 +626,19 @@ static int check_dead_slots(const GdfConfig& c, const double* uh) {
   return GDF_OK;
 }
 
-// Host-to-device copy of the 52 live slot planes of uh (the device copy's
-// dead slots are zero from allocation and no kernel writes them).
-static cudaError_t upload_live(double* dst, const double* uh, const GdfConfig& c, cudaStream_t st) {
+// Copy of the 52 live slot planes of uh (the device copies' dead slots are
+// zero from allocation and no kernel writes them).
+static cudaError_t copy_live(double* dst, const double* uh, const GdfConfig& c, cudaStream_t st,
+                             cudaMemcpyKind kind) {
   const size_t plane = (size_t)(c.nx + 2) * (c.ny + 2);
   for (int n = 0; n < NE; ++n) {
     // live slots of a variable are modes 0..5 plus (Bx) 6, 8 or (By) 7, 9
     const size_t o = plane * (10 * n);
-    cudaError_t e = cudaMemcpyAsync(dst + o, uh + o, 6 * plane * sizeof(double), cudaMemcpyHostToDevice, st);
+    cudaError_t e = cudaMemcpyAsync(dst + o, uh + o, 6 * plane * sizeof(double), kind, st);
     if (e != cudaSuccess) return e;
     for (int d = 6; d < NP; ++d) {
       if (!live_mode(n, d)) continue;
-      e = cudaMemcpyAsync(dst + o + plane * d, uh + o + plane * d, plane * sizeof(double), cudaMemcpyHostToDevice,
-                          st);
+      e = cudaMemcpyAsync(dst + o + plane * d, uh + o + plane * d, plane * sizeof(double), kind, st);
       if (e != cudaSuccess) return e;
     }
   }
@@ -780,9 +780,15 @@ int gdf_destroy(GdfHandle* h) {
 
 int gdf_upload(GdfHandle* h, const double* uh, const double* bx, const double* by) {
   if (!h || !uh || !bx || !by) return fail(GDF_ERR_ARG, "null argument");
+  // the live planes travel to a staging buffer while the host checks the
+  // dead ones; the resident state changes only once the check has passed
+  CK(copy_live(h->UT, uh, h->cfg, h->st, cudaMemcpyHostToDevice));
   int rc = check_dead_slots(h->cfg, uh);
-  if (rc) return rc;
-  CK(upload_live(h->U, uh, h->cfg, h->st));
+  if (rc) {
+    cudaStreamSynchronize(h->st);
+    return rc;
+  }
+  CK(copy_live(h->U, h->UT, h->cfg, h->st, cudaMemcpyDeviceToDevice));
   CK(cudaMemcpyAsync(h->BX, bx, bx_bytes(h->cfg), cudaMemcpyHostToDevice, h->st));
   CK(cudaMemcpyAsync(h->BY, by, by_bytes(h->cfg), cudaMemcpyHostToDevice, h->st));
   CK(cudaStreamSynchronize(h->st));
