@@ -29,6 +29,7 @@ KERNEL_SRC = os.path.join(CSRC, "gdf_kernels.cu")
 MLP_SRC = os.path.join(CSRC, "gdf_mlp.cu")
 ENS_SRC = os.path.join(CSRC, "gdf_ensemble.cu")
 HOST_SRC = os.path.join(CSRC, "gdf_host.cpp")
+IO_SRC = os.path.join(CSRC, "gdf_io.cpp")
 HEADERS = [os.path.join(CSRC, f) for f in ("gdf_physics.cuh", "gdf_kernels.cuh", "gdf_device.cuh",
                                                          "gdf_mlp.cuh")] + [
     os.path.join(REPO, "include", "gdf.h")]
@@ -60,9 +61,11 @@ def build(verbose: bool = False) -> dict:
     os.makedirs(BUILD, exist_ok=True)
     nvcc = _nvcc()
     host_o = os.path.join(BUILD, "gdf_host.o")
-    if _stale(host_o, [HOST_SRC] + HEADERS):
-        _run([HOST_CXX, "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-march=x86-64",
-              "-c", HOST_SRC, "-o", host_o])
+    io_o = os.path.join(BUILD, "gdf_io.o")
+    for src, obj in ((HOST_SRC, host_o), (IO_SRC, io_o)):
+        if _stale(obj, [src] + HEADERS):
+            _run([HOST_CXX, "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-march=x86-64",
+                  "-c", src, "-o", obj])
     out = {}
     for name, flags in (("libgdf_b200.so", ["--fmad=false", "-DGDF_EXACT=1"]),
                         ("libgdf_b200_fma.so", ["--fmad=true"])):
@@ -77,8 +80,8 @@ def build(verbose: bool = False) -> dict:
                 _run(cmd)
             objs.append(obj)
         so = os.path.join(LIB, name)
-        if _stale(so, objs + [host_o]):
-            _run([nvcc, *ARCH, "-shared", "-o", so, *objs, host_o])
+        if _stale(so, objs + [host_o, io_o]):
+            _run([nvcc, *ARCH, "-shared", "-o", so, *objs, host_o, io_o])
         out[name] = so
     return out
 

@@ -302,4 +302,60 @@ int gdf_init_data(const GdfConfig* cfg, int32_t problem, const double* params, d
   return GDF_OK;
 }
 
+// calculate_L2error.f90:1-38: L2 norms per variable of the numerical
+// solution minus the vortex of init1.txt moved by (t20, t20), on the 5x5
+// Gauss points of every cell, in the reference's loop and summation order.
+int gdf_l2_error(const GdfConfig* cfg, const double* uh, double t20, double* L2) {
+  if (!cfg || !uh || !L2 || cfg->nx < 1 || cfg->ny < 1) return GDF_ERR_ARG;
+  Init P;
+  P.problem = GDF_PROB_VORTEX;
+  P.g = cfg->gamma;
+  default_params(GDF_PROB_VORTEX, P.prm);
+  const int Nx = cfg->nx, Ny = cfg->ny;
+  const double hx = (cfg->xb - cfg->xa) / Nx, hy = (cfg->yb - cfg->ya) / Ny;
+  const double hx1 = 0.5 * hx, hy1 = 0.5 * hy;
+  const size_t NX2 = (size_t)Nx + 2, NY2 = (size_t)Ny + 2;
+  const double c13 = 1.0 / 3.0, c35 = 3.0 / 5.0;
+  auto phi = [&](double li, double lj, int d) {
+    switch (d) {
+      case 0: return 1.0;
+      case 1: return li;
+      case 2: return lj;
+      case 3: return li * li - c13;
+      case 4: return li * lj;
+      case 5: return lj * lj - c13;
+      case 6: return li * li * li - c35 * li;
+      case 7: return (li * li - c13) * lj;
+      case 8: return li * (lj * lj - c13);
+      default: return lj * lj * lj - c35 * lj;
+    }
+  };
+  double acc[NE] = {0, 0, 0, 0, 0, 0, 0, 0};
+  double Uv[NE];
+  for (int i = 1; i <= Nx; ++i)
+    for (int j = 1; j <= Ny; ++j) {
+      double uG[NG][NG][NE];
+      for (int a = 0; a < NG; ++a)
+        for (int b = 0; b < NG; ++b)
+          for (int n = 0; n < NE; ++n) uG[a][b][n] = 0.0;
+      for (int n = 0; n < NE; ++n)
+        for (int d = 0; d < NP; ++d) {
+          const double m = uh[i + NX2 * (j + NY2 * (d + 10 * (size_t)n))];
+          for (int a = 0; a < NG; ++a)
+            for (int b = 0; b < NG; ++b) uG[a][b][n] = uG[a][b][n] + m * phi(kLam[a], kLam[b], d);
+        }
+      const double xc = cfg->xa + (i - 0.5) * hx, yc = cfg->ya + (j - 0.5) * hy;
+      for (int a = 0; a < NG; ++a)
+        for (int b = 0; b < NG; ++b) {
+          P.conserved(xc + hx1 * kLam[a] - t20, yc + hy1 * kLam[b] - t20, Uv);
+          for (int n = 0; n < NE; ++n) {
+            const double e = uG[a][b][n] - Uv[n];
+            acc[n] = acc[n] + kW[a] * kW[b] * (e * e);
+          }
+        }
+    }
+  for (int n = 0; n < NE; ++n) L2[n] = std::sqrt(acc[n] * hx1 * hy1);
+  return GDF_OK;
+}
+
 }  // extern "C"

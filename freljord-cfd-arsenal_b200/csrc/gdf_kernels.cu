@@ -464,6 +464,8 @@ static int check_config(const GdfConfig* c) {
 }
 
 namespace gdf {
+// the message gdf_last_error() returns, for the host-only parts of the ABI
+int set_last_error(int code, const char* msg) { return fail(code, msg); }
 void consts_for(const GdfConfig& c, Consts& K) { build_consts(c, K); }
 void basis_of(const Consts& K, Basis& B) {
   std::memcpy(B.w, K.w, sizeof(B.w));
@@ -987,6 +989,29 @@ int gdf_features(GdfHandle* h, const double* uh, float* X) {
   cudaFreeAsync(dX, h->st);
   CK(cudaStreamSynchronize(h->st));
   return rc;
+}
+
+int gdf_config_of(GdfHandle* h, GdfConfig* out) {
+  if (!h || !out) return fail(GDF_ERR_ARG, "null argument");
+  *out = h->cfg;
+  return GDF_OK;
+}
+
+// Is_Trouble_Cell (the sticky KXRCF flags), nx*ny int32 in (i-1)+nx*(j-1) order
+int gdf_get_trouble(GdfHandle* h, int32_t* trouble) {
+  if (!h || !trouble) return fail(GDF_ERR_ARG, "null argument");
+  CK(cudaMemcpyAsync(trouble, h->trouble, (size_t)h->cfg.nx * h->cfg.ny * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                     h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return GDF_OK;
+}
+
+int gdf_set_trouble(GdfHandle* h, const int32_t* trouble) {
+  if (!h || !trouble) return fail(GDF_ERR_ARG, "null argument");
+  CK(cudaMemcpyAsync(h->trouble, trouble, (size_t)h->cfg.nx * h->cfg.ny * sizeof(int32_t), cudaMemcpyHostToDevice,
+                     h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return GDF_OK;
 }
 
 int gdf_set_device(int32_t device) {

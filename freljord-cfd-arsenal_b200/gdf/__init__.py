@@ -88,6 +88,16 @@ def load(exact: bool = True):
     L.gdf_advance_timed.argtypes = [vp, C.c_double, i32, dp, ip, dp]
     L.gdf_set_device.argtypes = [i32]
     L.gdf_lh_noalloc.argtypes = [cfgp, vp, vp, vp]
+    cp = C.c_char_p
+    L.gdf_save_solution.argtypes = [cfgp, dp, cp]
+    L.gdf_save_frame.argtypes = [cfgp, dp, C.c_double, cp, i32]
+    L.gdf_save_xy.argtypes = [cfgp, cp]
+    L.gdf_l2_error.argtypes = [cfgp, dp, C.c_double, dp]
+    L.gdf_config_of.argtypes = [vp, cfgp]
+    L.gdf_get_trouble.argtypes = [vp, ip]
+    L.gdf_set_trouble.argtypes = [vp, ip]
+    L.gdf_checkpoint_save.argtypes = [vp, cp]
+    L.gdf_checkpoint_load.argtypes = [vp, cp]
     fp = C.POINTER(C.c_float)
     L.gdf_features.argtypes = [vp, dp, fp]
     L.gdf_mlp_create.argtypes = [i32, C.POINTER(vp)]
@@ -153,6 +163,33 @@ def init_data(cfg: GdfConfig, problem: int, params=None, exact: bool = True):
     p = None if params is None else dptr(np.ascontiguousarray(params, np.float64))
     _check(L, L.gdf_init_data(C.byref(cfg), problem, p, dptr(uh), dptr(bx), dptr(by)))
     return uh, bx, by
+
+
+def save_solution(cfg: GdfConfig, uh, directory: str = ".", exact: bool = True) -> None:
+    """save_solution.f90: Q1.txt..Q8.txt of uh in directory."""
+    L = load(exact)
+    _check(L, L.gdf_save_solution(C.byref(cfg), dptr(uh), directory.encode()))
+
+
+def save_frame(cfg: GdfConfig, uh, t: float, directory: str = ".", reset: bool = False,
+               exact: bool = True) -> None:
+    """One frame of RK3.f90's Q*flash.txt / T.txt output (reset: new files)."""
+    L = load(exact)
+    _check(L, L.gdf_save_frame(C.byref(cfg), dptr(uh), t, directory.encode(), 1 if reset else 0))
+
+
+def save_xy(cfg: GdfConfig, directory: str = ".", exact: bool = True) -> None:
+    """save_XY.f90: Xc.txt, Yc.txt, lambda.txt, weight.txt."""
+    L = load(exact)
+    _check(L, L.gdf_save_xy(C.byref(cfg), directory.encode()))
+
+
+def l2_error(cfg: GdfConfig, uh, t20: float = 0.0, exact: bool = True) -> np.ndarray:
+    """calculate_L2error.f90 against the vortex of init1.txt moved by (t20, t20)."""
+    L = load(exact)
+    out = np.zeros(NE)
+    _check(L, L.gdf_l2_error(C.byref(cfg), dptr(uh), t20, dptr(out)))
+    return out
 
 
 class Solver:
@@ -269,6 +306,25 @@ class Solver:
 
     def kernel_launches(self) -> int:
         return self.L.gdf_kernel_launches(self.h)
+
+    def trouble(self):
+        """The sticky KXRCF flags (Is_Trouble_Cell), shape (ny, nx)."""
+        f = self._flags()
+        _check(self.L, self.L.gdf_get_trouble(self.h, iptr(f)))
+        return f
+
+    def set_trouble(self, f) -> None:
+        f = np.ascontiguousarray(f, np.int32)
+        _check(self.L, self.L.gdf_set_trouble(self.h, iptr(f)))
+
+    def checkpoint(self, path: str) -> None:
+        """gdf_checkpoint_save: state, time and sticky flags to a file."""
+        _check(self.L, self.L.gdf_checkpoint_save(self.h, os.fsencode(path)))
+
+    def restore(self, path: str) -> None:
+        """gdf_checkpoint_load into this handle (same configuration)."""
+        _check(self.L, self.L.gdf_checkpoint_load(self.h, os.fsencode(path)))
+        self.t = self.time()[0]
 
     def stream(self) -> int:
         """The handle's cudaStream_t as an integer."""

@@ -309,6 +309,38 @@ enum {
 int gdf_profile(GdfHandle *h, int32_t steps, double *ms_per_launch,
                 int64_t *launches_per_kind, int32_t nkinds);
 
+/* ---- output files, error norm and checkpoint (main.f90's flow) -------- */
+/* save_solution.f90: Q1.txt..Q8.txt in dir (NULL or "" = current
+ * directory), uh(i,j,d,n) of the interior cells, one value per line in the
+ * reference's order (d, then j, then i), 17 significant digits. */
+int gdf_save_solution(const GdfConfig *cfg, const double *uh, const char *dir);
+/* RK3.f90:29-53,154-172: one frame appended to Q1flash.txt..Q8flash.txt and
+ * its time to T.txt (reset = 1 starts the files afresh, as RK3's first
+ * frame does). The caller decides when a frame is due: the reference writes
+ * the state after prepare and then whenever t > (tend/frameMAX)*countf or
+ * t == tend. */
+int gdf_save_frame(const GdfConfig *cfg, const double *uh, double t, const char *dir, int32_t reset);
+/* save_XY.f90: Xc.txt, Yc.txt (Gauss point coordinates of every column /
+ * row of cells), lambda.txt, weight.txt. */
+int gdf_save_xy(const GdfConfig *cfg, const char *dir);
+/* calculate_L2error.f90: L2[8] = the L2 norms per variable of uh minus the
+ * smooth vortex of init1.txt moved by (t20, t20) (main.f90 passes t20 =
+ * tend when tend <= 5, else 0). Host only. */
+int gdf_l2_error(const GdfConfig *cfg, const double *uh, double t20, double *L2);
+/* The handle's configuration. */
+int gdf_config_of(GdfHandle *h, GdfConfig *out);
+/* Is_Trouble_Cell of KXRCF_Detector.f90: the sticky flags, int32
+ * trouble(1:Nx,1:Ny) in Fortran order. */
+int gdf_get_trouble(GdfHandle *h, int32_t *trouble);
+int gdf_set_trouble(GdfHandle *h, const int32_t *trouble);
+/* Binary checkpoint of a handle (no counterpart in the reference, which
+ * cannot restart): configuration, t, dt, uh, Bx, By and the sticky flags.
+ * Loading into a handle of the same configuration restores a run that then
+ * continues value for value as if uninterrupted; another configuration or
+ * a damaged file gives GDF_ERR_ARG. */
+int gdf_checkpoint_save(GdfHandle *h, const char *path);
+int gdf_checkpoint_load(GdfHandle *h, const char *path);
+
 /* Message of the last failure on this thread ("" if none). */
 const char *gdf_last_error(void);
 
