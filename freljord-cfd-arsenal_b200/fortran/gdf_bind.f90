@@ -84,5 +84,44 @@ module gdf_bind
     type(c_ptr) function gdf_last_error() bind(c, name="gdf_last_error")
       import :: c_ptr
     end function
+    ! output files of save_solution.f90 / RK3.f90 frames / save_XY.f90,
+    ! calculate_L2error.f90, and the binary checkpoint (dir, path: C strings,
+    ! e.g. "out"//c_null_char)
+    integer(c_int) function gdf_save_solution(cfg, uh, dir) bind(c, name="gdf_save_solution")
+      import :: c_int, c_double, c_char, gdf_config
+      type(gdf_config), intent(in) :: cfg
+      real(c_double), intent(in) :: uh(*)
+      character(kind=c_char), intent(in) :: dir(*)
+    end function
+    integer(c_int) function gdf_save_frame(cfg, uh, t, dir, reset) bind(c, name="gdf_save_frame")
+      import :: c_int, c_double, c_char, gdf_config
+      type(gdf_config), intent(in) :: cfg
+      real(c_double), intent(in) :: uh(*)
+      real(c_double), value :: t
+      character(kind=c_char), intent(in) :: dir(*)
+      integer(c_int), value :: reset
+    end function
+    integer(c_int) function gdf_save_xy(cfg, dir) bind(c, name="gdf_save_xy")
+      import :: c_int, c_char, gdf_config
+      type(gdf_config), intent(in) :: cfg
+      character(kind=c_char), intent(in) :: dir(*)
+    end function
+    integer(c_int) function gdf_l2_error(cfg, uh, t20, l2) bind(c, name="gdf_l2_error")
+      import :: c_int, c_double, gdf_config
+      type(gdf_config), intent(in) :: cfg
+      real(c_double), intent(in) :: uh(*)
+      real(c_double), value :: t20
+      real(c_double), intent(out) :: l2(8)
+    end function
+    integer(c_int) function gdf_checkpoint_save(h, path) bind(c, name="gdf_checkpoint_save")
+      import :: c_int, c_ptr, c_char
+      type(c_ptr), value :: h
+      character(kind=c_char), intent(in) :: path(*)
+    end function
+    integer(c_int) function gdf_checkpoint_load(h, path) bind(c, name="gdf_checkpoint_load")
+      import :: c_int, c_ptr, c_char
+      type(c_ptr), value :: h
+      character(kind=c_char), intent(in) :: path(*)
+    end function
   end interface
 end module gdf_bind
