@@ -64,7 +64,7 @@ def build(verbose: bool = False) -> dict:
     io_o = os.path.join(BUILD, "gdf_io.o")
     for src, obj in ((HOST_SRC, host_o), (IO_SRC, io_o)):
         if _stale(obj, [src] + HEADERS):
-            _run([HOST_CXX, "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-march=x86-64",
+            _run([HOST_CXX, "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-march=x86-64", "-fopenmp",
                   "-c", src, "-o", obj])
     out = {}
     for name, flags in (("libgdf_b200.so", ["--fmad=false", "-DGDF_EXACT=1"]),
@@ -81,7 +81,7 @@ def build(verbose: bool = False) -> dict:
             objs.append(obj)
         so = os.path.join(LIB, name)
         if _stale(so, objs + [host_o, io_o]):
-            _run([nvcc, *ARCH, "-shared", "-o", so, *objs, host_o, io_o])
+            _run([nvcc, *ARCH, "-shared", "-o", so, *objs, host_o, io_o, "-Xcompiler", "-fopenmp", "-lgomp"])
         out[name] = so
     return out
 

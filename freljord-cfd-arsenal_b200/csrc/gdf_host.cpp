@@ -242,45 +242,63 @@ int gdf_init_data(const GdfConfig* cfg, int32_t problem, const double* params, d
   const double mmE[3] = {1, 1.0 / 3.0, 4.0 / 45.0};
   double Uv[NE];
   if (!shock) {
+    // cells are independent: spread them over the host threads (the values
+    // do not depend on the split)
+#pragma omp parallel for schedule(dynamic, 4)
     for (int i = 1; i <= Nx; ++i)
       for (int j = 1; j <= Ny; ++j) {
-        // init_data.f90:37-63: only modes 1..6 pass the projection mask
+        // the point values once per cell, then init_data.f90:37-63 (only
+        // modes 1..6 pass the projection mask), summed in the same order
+        double Up[NG][NG][NE];
+        for (int a = 0; a < NG; ++a)
+          for (int b = 0; b < NG; ++b) P.conserved(Xc[i] + hx1 * kLam[a], Yc[j] + hy1 * kLam[b], Up[a][b]);
         double acc[6][NE];
         for (int d = 0; d < 6; ++d)
           for (int n = 0; n < NE; ++n) acc[d][n] = 0.0;
         for (int d = 0; d < 6; ++d)
           for (int a = 0; a < NG; ++a)
             for (int b = 0; b < NG; ++b) {
-              P.conserved(Xc[i] + hx1 * kLam[a], Yc[j] + hy1 * kLam[b], Uv);
               const double f = kW[a] * kW[b] * phiG(a, b, d);
-              for (int n = 0; n < NE; ++n) acc[d][n] = acc[d][n] + f * Uv[n];
+              for (int n = 0; n < NE; ++n) acc[d][n] = acc[d][n] + f * Up[a][b][n];
             }
         for (int d = 0; d < 6; ++d)
           for (int n = 0; n < NE; ++n) U(i, j, d, n) = 0.25 * acc[d][n] / mm[d];
       }
     // face projections of Bx and By (init_data.f90:65-90)
+#pragma omp parallel for schedule(dynamic, 4)
     for (int i = 0; i <= Nx; ++i)
-      for (int j = 1; j <= Ny; ++j)
+      for (int j = 1; j <= Ny; ++j) {
+        double Bq[NG], Uq[NE];
+        for (int b = 0; b < NG; ++b) {
+          P.conserved(cfg->xa + i * hx, Yc[j] + hy1 * kLam[b], Uq);
+          Bq[b] = Uq[5];
+        }
         for (int d = 0; d < 3; ++d) {
           double acc = 0.0;
           for (int b = 0; b < NG; ++b) {
-            P.conserved(cfg->xa + i * hx, Yc[j] + hy1 * kLam[b], Uv);
             const double e = d == 0 ? 1.0 : d == 1 ? kLam[b] : kLam[b] * kLam[b] - c13;
-            acc = acc + 0.5 * kW[b] * e * Uv[5];
+            acc = acc + 0.5 * kW[b] * e * Bq[b];
           }
           bx[i + (size_t)(Nx + 1) * ((j - 1) + (size_t)Ny * d)] = acc / mmE[d];
         }
+      }
+#pragma omp parallel for schedule(dynamic, 4)
     for (int i = 1; i <= Nx; ++i)
-      for (int j = 0; j <= Ny; ++j)
+      for (int j = 0; j <= Ny; ++j) {
+        double Bq[NG], Uq[NE];
+        for (int a = 0; a < NG; ++a) {
+          P.conserved(Xc[i] + hx1 * kLam[a], cfg->ya + j * hy, Uq);
+          Bq[a] = Uq[6];
+        }
         for (int d = 0; d < 3; ++d) {
           double acc = 0.0;
           for (int a = 0; a < NG; ++a) {
-            P.conserved(Xc[i] + hx1 * kLam[a], cfg->ya + j * hy, Uv);
             const double e = d == 0 ? 1.0 : d == 1 ? kLam[a] : kLam[a] * kLam[a] - c13;
-            acc = acc + 0.5 * kW[a] * e * Uv[6];
+            acc = acc + 0.5 * kW[a] * e * Bq[a];
           }
           by[(i - 1) + (size_t)Nx * (j + (size_t)(Ny + 1) * d)] = acc / mmE[d];
         }
+      }
   } else {
     // shock == 1 (init_data.f90:92-121): point values, higher modes zero
     for (int i = 1; i <= Nx; ++i)
