@@ -810,8 +810,67 @@ __device__ __forceinline__ bool lim_gate(const Consts& K, const double* __restri
   return gate;
 }
 
+// TVB_Limiter_P1.f90:19-90: characteristic minmod of the two slopes only;
+// a changed variable keeps its limited slopes and loses every higher mode
+__device__ __forceinline__ void lim_tvb_p1(const Consts& K, const double* __restrict__ S, long long c,
+                                           double (*m)[NP], int32_t& word) {
+  const long long pl = K.plane;
+  const double rhoij = m[0][0];
+  const double u1 = m[1][0] / rhoij, u2 = m[2][0] / rhoij, u3 = m[3][0] / rhoij;
+  const double Eij = m[4][0], B1 = m[5][0], B2 = m[6][0], B3 = m[7][0];
+  double R[64], L[64];
+  double DR[NE], DL[NE], D1[NE], t1[NE], t2[NE], tu[NE], mod[NE], Xm[NE], Ym[NE];
+  unsigned change = 0;
+  eigenmatrix(K.P, 0, rhoij, u1, u2, u3, Eij, B1, B2, B3, R, L);
+#pragma unroll
+  for (int n = 0; n < NE; ++n) {
+    DR[n] = S[c + 1 + pl * (10 * n)] - m[n][0];
+    DL[n] = m[n][0] - S[c - 1 + pl * (10 * n)];
+    D1[n] = m[n][1];
+  }
+  matvec8(L, DR, t1);
+  matvec8(L, DL, t2);
+  matvec8(L, D1, tu);
+#pragma unroll
+  for (int k = 0; k < NE; ++k) mod[k] = minmod1(tu[k], t1[k], t2[k], K.Mh2x);
+  matvec8(R, mod, Xm);
+#pragma unroll
+  for (int d = 0; d < NE; ++d)
+    if (fabs(Xm[d] - D1[d]) > 1e-6) change |= 1u << d;
+  eigenmatrix(K.P, 1, rhoij, u1, u2, u3, Eij, B1, B2, B3, R, L);
+#pragma unroll
+  for (int n = 0; n < NE; ++n) {
+    DR[n] = S[c + K.nx2 + pl * (10 * n)] - m[n][0];
+    DL[n] = m[n][0] - S[c - K.nx2 + pl * (10 * n)];
+    D1[n] = m[n][2];
+  }
+  matvec8(L, DR, t1);
+  matvec8(L, DL, t2);
+  matvec8(L, D1, tu);
+#pragma unroll
+  for (int k = 0; k < NE; ++k) mod[k] = minmod1(tu[k], t1[k], t2[k], K.Mh2y);
+  matvec8(R, mod, Ym);
+#pragma unroll
+  for (int d = 0; d < NE; ++d)
+    if (fabs(Ym[d] - D1[d]) > 1e-6) change |= 1u << d;
+#pragma unroll
+  for (int n = 0; n < NE; ++n) {
+    if (change & (1u << n)) {
+#pragma unroll
+      for (int d = 3; d < NP; ++d) m[n][d] = 0.0;
+      m[n][1] = Xm[n];
+      m[n][2] = Ym[n];
+    }
+  }
+  word |= (int32_t)change;
+}
+
 __device__ __forceinline__ void lim_tvb(const Consts& K, const double* __restrict__ S, long long c,
                                         double (*m)[NP], int32_t& word) {
+  if (K.tvb_p1) {
+    lim_tvb_p1(K, S, c, m, word);
+    return;
+  }
   const long long pl = K.plane;
     const double c23 = 2.0 / 3.0;
     const double rhoij = m[0][0];

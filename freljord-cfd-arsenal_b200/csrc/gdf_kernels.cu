@@ -369,7 +369,9 @@ static void build_consts(const GdfConfig& c, Consts& K) {
   K.ck = c.kxrcf_ck;
   K.pow_hxhy = std::pow(K.hx * K.hy, 0.25 * (2 + 1));  // KXRCF_Detector.f90:98
   K.bc_r = c.bc_r; K.bc_l = c.bc_l; K.bc_u = c.bc_u; K.bc_d = c.bc_d;
-  K.pp = c.pp_limiter; K.faceb = c.faceb_limiter; K.ez_fhat = c.ez_face_fhat;
+  // TVB_Limiter_P1.f90:113-164 applies the face-B minmod whatever the switch
+  K.pp = c.pp_limiter; K.faceb = (c.faceb_limiter || c.tvb_p1) ? 1 : 0; K.ez_fhat = c.ez_face_fhat;
+  K.tvb_p1 = c.tvb_p1;
   K.eig_y_zero_w = c.eig_y_zero_w; K.detector = c.detector; K.sticky = c.kxrcf_sticky;
   K.dt_floor_stop = c.dt_floor_stop; K.umax_all = c.umax_all_vars;
   K.P.gamma = c.gamma;

@@ -39,6 +39,7 @@ struct Consts {
   double tvb_slope, cfl, ck, pow_hxhy;
   int bc_r, bc_l, bc_u, bc_d;
   int pp, faceb, ez_fhat, eig_y_zero_w, detector, sticky, dt_floor_stop, umax_all;
+  int tvb_p1;               // TVB_Limiter_P1 in place of TVB_Limiter_P2
   double w[NG], lam[NG];
   double phiG[NG][NG][NP], phix[NG][NG][NP], phiy[NG][NG][NP];
   double phiGLL[2][NG][NG][NP];

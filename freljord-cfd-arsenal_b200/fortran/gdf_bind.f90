@@ -24,7 +24,8 @@ module gdf_bind
     integer(c_int32_t) :: eig_y_zero_w, kml_w_term, dt_floor_stop, umax_all_vars, detector
     real(c_double)     :: kxrcf_ck
     integer(c_int32_t) :: kxrcf_sticky
-    integer(c_int32_t) :: reserved_i(7)
+    integer(c_int32_t) :: tvb_p1
+    integer(c_int32_t) :: reserved_i(6)
     real(c_double)     :: reserved_d(4)
   end type gdf_config
 

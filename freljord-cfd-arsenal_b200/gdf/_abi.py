@@ -42,7 +42,7 @@ class GdfConfig(C.Structure):
         ("detector", C.c_int32),
         ("kxrcf_ck", C.c_double),
         ("kxrcf_sticky", C.c_int32),
-        ("reserved_i", C.c_int32 * 7),
+        ("tvb_p1", C.c_int32), ("reserved_i", C.c_int32 * 6),
         ("reserved_d", C.c_double * 4),
     ]
 

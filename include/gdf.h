@@ -101,7 +101,10 @@ typedef struct GdfConfig {
   int32_t detector;          /* GDF_DETECT_*                                    */
   double kxrcf_ck;           /* KXRCF_Detector.f90:7 threshold Ck              */
   int32_t kxrcf_sticky;      /* KXRCF flags never reset (Is_Trouble_Cell)      */
-  int32_t reserved_i[7];
+  int32_t tvb_p1;            /* TVB_Limiter_P1.f90 in place of TVB_Limiter_P2:
+                                the two slopes only, higher modes zeroed where
+                                changed, face-B minmod always applied       */
+  int32_t reserved_i[6];
   double reserved_d[4];
 } GdfConfig;
 

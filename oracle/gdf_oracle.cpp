@@ -1382,6 +1382,47 @@ struct Oracle {
           double R[64], L[64];
           double DR[NE], DL[NE], D1p[NE], D1m[NE], t1[NE], t2[NE], tU[NE], mod[NE];
           double Rp[NE], Rm[NE], Up[NE], Um[NE];
+          if (c.tvb_p1) {
+            // TVB_Limiter_P1.f90:19-90: slopes only; a changed variable keeps
+            // its limited slopes and loses every higher mode
+            double Xm[NE], Ym[NE], D1[NE];
+            eigenmatrix(R, L, rhoij, u1ij, u2ij, u3ij, Eij, B1ij, B2ij, B3ij, 1.0, 0.0, 0.0);
+            for (int n = 1; n <= NE; ++n) {
+              DR[n - 1] = uh[U(i + 1, j, 1, n)] - uh[U(i, j, 1, n)];
+              DL[n - 1] = uh[U(i, j, 1, n)] - uh[U(i - 1, j, 1, n)];
+              D1[n - 1] = uh[U(i, j, 2, n)];
+            }
+            matvec(L, DR, t1);
+            matvec(L, DL, t2);
+            matvec(L, D1, tU);
+            minmod(tU, t1, t2, M, hx, mod);
+            matvec(R, mod, Xm);
+            for (int d = 0; d < NE; ++d)
+              if (std::fabs(Xm[d] - D1[d]) > 1e-6) change[d] = 1;
+            eigenmatrix(R, L, rhoij, u1ij, u2ij, u3ij, Eij, B1ij, B2ij, B3ij, 0.0, 1.0, 0.0);
+            for (int n = 1; n <= NE; ++n) {
+              DR[n - 1] = uh[U(i, j + 1, 1, n)] - uh[U(i, j, 1, n)];
+              DL[n - 1] = uh[U(i, j, 1, n)] - uh[U(i, j - 1, 1, n)];
+              D1[n - 1] = uh[U(i, j, 3, n)];
+            }
+            matvec(L, DR, t1);
+            matvec(L, DL, t2);
+            matvec(L, D1, tU);
+            minmod(tU, t1, t2, M, hy, mod);
+            matvec(R, mod, Ym);
+            for (int d = 0; d < NE; ++d)
+              if (std::fabs(Ym[d] - D1[d]) > 1e-6) change[d] = 1;
+            for (int d = 1; d <= NE; ++d) {
+              if (change[d - 1] == 1) {
+                word |= (1 << (d - 1));
+                for (int q = 4; q <= NP; ++q) uhmod[U(i, j, q, d)] = 0;
+                uhmod[U(i, j, 2, d)] = Xm[d - 1];
+                uhmod[U(i, j, 3, d)] = Ym[d - 1];
+              }
+            }
+            if (flags) flags[cell] = word;
+            continue;
+          }
           // x direction (:35-68)
           eigenmatrix(R, L, rhoij, u1ij, u2ij, u3ij, Eij, B1ij, B2ij, B3ij, 1.0, 0.0, 0.0);
           for (int n = 1; n <= NE; ++n) {
@@ -1443,7 +1484,7 @@ struct Oracle {
     par_copy(uhmod.data(), uh, uhsize());
     if (c.pp_limiter) pp_limiter(uh);
     set_bc(uh);
-    if (c.faceb_limiter) {
+    if (c.faceb_limiter || c.tvb_p1) {   // TVB_Limiter_P1 applies it always
       // TVB_Limiter_P2.f90:128-187 (face traces of cell B from both sides,
       // minmodB of face modes 2..3, applied)
       const double c25 = 2.0 / 5.0;

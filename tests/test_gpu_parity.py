@@ -199,6 +199,10 @@ VARIANTS = {
     "kxrcf_nonsticky": lambda c: (setattr(c, "detector", gdf.DETECT_KXRCF), setattr(c, "kxrcf_ck", 0.5),
                                   setattr(c, "kxrcf_sticky", 0)),
     "consistent_gamma": lambda c: setattr(c, "gamma_flux", c.gamma),
+    # TVB_Limiter_P1 in place of TVB_Limiter_P2 (slopes only, face-B minmod)
+    "p1_limiter": lambda c: setattr(c, "tvb_p1", 1),
+    "p1_limiter_kxrcf_pp": lambda c: (setattr(c, "tvb_p1", 1), setattr(c, "detector", gdf.DETECT_KXRCF),
+                                      setattr(c, "kxrcf_ck", 0.5), setattr(c, "pp_limiter", 1)),
 }
 
 

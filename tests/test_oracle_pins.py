@@ -197,3 +197,34 @@ def test_smooth_vortex_third_order():
     order = np.log2(errs[0] / errs[1])
     for var in (0, 1, 2, 4, 5, 6):
         assert order[var] > 2.6, (var, order)
+
+
+def test_p1_limiter_limits_slopes_only():
+    """TVB_Limiter_P1: a limited variable keeps its two slopes (limited) and
+    loses every higher mode; unlimited variables are untouched; the face-B
+    minmod applies whatever faceb_limiter says."""
+    import gdf
+    from oracle import Oracle
+    cfg, _ = gdf.problem_config(gdf.PROB_BLAST, 16, 16)
+    cfg.tvb_p1 = 1
+    cfg.faceb_limiter = 0
+    cfg.pp_limiter = 0
+    cfg.detector = gdf.DETECT_ALL
+    o = Oracle(cfg)
+    uh, bx, by = o.init_data(gdf.PROB_BLAST)
+    o.set_bc(uh)
+    du = o.lh(uh)
+    d1, d2 = o.lhez(uh)
+    dt = o.dt(uh)
+    u = uh + dt * du
+    b, c = bx + dt * d1, by + dt * d2
+    before = u.copy()
+    f = o.limit(u, b, c)
+    changed = (f & 0xFF) != 0
+    assert changed.any()
+    for n in (0, 1, 2, 3, 4, 7):             # B is rebuilt by the div-free step
+        mask = ((f >> n) & 1).astype(bool)
+        cells = u[n, :, 1:-1, 1:-1]
+        assert np.all(cells[3:, mask] == 0)  # higher modes dropped
+        assert np.all(cells[0] == before[n, 0, 1:-1, 1:-1])   # means kept
+        assert np.array_equal(cells[:, ~mask], before[n, :, 1:-1, 1:-1][:, ~mask])
