@@ -810,6 +810,16 @@ int gdf_download(GdfHandle* h, double* uh, double* bx, double* by) {
   return GDF_OK;
 }
 
+int gdf_download_live(GdfHandle* h, double* uh, double* bx, double* by) {
+  if (!h) return fail(GDF_ERR_ARG, "null handle");
+  if (!h->uploaded) return fail(GDF_ERR_STATE, "no state uploaded");
+  if (uh) CK(copy_live(uh, h->U, h->cfg, h->st, cudaMemcpyDeviceToHost));
+  if (bx) CK(cudaMemcpyAsync(bx, h->BX, bx_bytes(h->cfg), cudaMemcpyDeviceToHost, h->st));
+  if (by) CK(cudaMemcpyAsync(by, h->BY, by_bytes(h->cfg), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return GDF_OK;
+}
+
 int gdf_set_time(GdfHandle* h, double t) {
   if (!h) return fail(GDF_ERR_ARG, "null handle");
   int rc = sync_scal(h);

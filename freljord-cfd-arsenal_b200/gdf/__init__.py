@@ -70,6 +70,7 @@ def load(exact: bool = True):
     L.gdf_destroy.argtypes = [vp]
     L.gdf_upload.argtypes = [vp, dp, dp, dp]
     L.gdf_download.argtypes = [vp, dp, dp, dp]
+    L.gdf_download_live.argtypes = [vp, dp, dp, dp]
     L.gdf_prepare.argtypes = [vp, ip]
     L.gdf_step.argtypes = [vp, C.c_double, dp, dp, ip]
     L.gdf_advance.argtypes = [vp, C.c_double, i32, dp, ip]
@@ -235,9 +236,11 @@ class Solver:
     def set_indicator(self, mlp: "Mlp", t_lo: float = 0.5, t_hi: float = 0.5) -> None:
         _check(self.L, self.L.gdf_set_indicator(self.h, mlp.h, t_lo, t_hi))
 
-    def download_into(self, uh, bx, by) -> None:
-        """gdf_download into caller arrays (e.g. pinned host buffers)."""
-        _check(self.L, self.L.gdf_download(self.h, dptr(uh), dptr(bx), dptr(by)))
+    def download_into(self, uh, bx, by, live_only: bool = False) -> None:
+        """gdf_download into caller arrays (e.g. pinned host buffers);
+        live_only: gdf_download_live (dead slot planes of uh not written)."""
+        f = self.L.gdf_download_live if live_only else self.L.gdf_download
+        _check(self.L, f(self.h, dptr(uh), dptr(bx), dptr(by)))
 
     def prepare(self):
         f = self._flags()

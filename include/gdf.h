@@ -136,6 +136,12 @@ int gdf_destroy(GdfHandle *h);
 /* Copy the full reference arrays to / from the device (synchronous). */
 int gdf_upload(GdfHandle *h, const double *uh, const double *bx, const double *by);
 int gdf_download(GdfHandle *h, double *uh, double *bx, double *by);
+/* As gdf_download, but only the 52 live (mode, variable) planes of uh are
+ * written; the 28 dead ones of the caller's array are left as they are (the
+ * P2 scheme never populates them, so a host that keeps one uh array, as the
+ * reference's COMMON block, already holds zeros there). 35% less
+ * device-to-host traffic per call. No counterpart in the reference. */
+int gdf_download_live(GdfHandle *h, double *uh, double *bx, double *by);
 
 /* RK3.f90:5-12: t = 0, set_bc, TVB_Limiter_P2, div_free_Balsara on the
  * resident state. flags (may be NULL) receives the troubled-cell word of

@@ -137,3 +137,23 @@ def test_main_driver_writes_the_reference_files(tmp_path):
         assert os.path.exists(os.path.join(out, name))
     q1 = np.loadtxt(os.path.join(out, "Q1flash.txt")).reshape(frames.size, -1)
     assert np.array_equal(q1[-1], np.loadtxt(os.path.join(out, "Q1.txt")))
+
+
+@pytest.mark.gpu
+def test_download_live_writes_only_live_planes():
+    cfg, tend, uh, bx, by = small_state(gdf.PROB_ROTOR, 20, 16)
+    s = gdf.Solver(cfg)
+    s.upload(uh, bx, by)
+    s.prepare()
+    s.advance(tend, 2)
+    full = s.download()
+    marked = np.full_like(uh, 7.0)
+    b1, b2 = np.zeros_like(bx), np.zeros_like(by)
+    s.download_into(marked, b1, b2, live_only=True)
+    live = np.zeros((8, 10), bool)
+    live[:, :6] = True
+    live[5, [6, 8]] = True
+    live[6, [7, 9]] = True
+    assert np.array_equal(marked[live], full[0][live])
+    assert np.all(marked[~live] == 7.0)
+    assert np.array_equal(b1, full[1]) and np.array_equal(b2, full[2])
