@@ -36,7 +36,8 @@ WORKLOAD = ("MHD rotor 512x512 on [0,1]^2, P2 modal DG FP64 (8 vars x 10 modal s
             "div-free B, SSP-RK3, CFL 0.15 (plain method)")
 
 # Compulsory HBM bytes per cell for one launch of each kernel kind (FP64,
-# 52 live modal slots = 416 B per cell state). See DESIGN.md "roofline".
+# 52 live modal slots = 416 B per cell state): what one launch must read
+# and write at least, stage mean for the residual kernel.
 ALG_BYTES_PER_CELL = {
     "face_x": 416 + 40 * 8 + 5 * 8,          # cell modes once, Fxhat + EzRL of the cell's face
     "face_y": 416 + 40 * 8 + 5 * 8,
