@@ -15,9 +15,10 @@
 // Per instance, a step runs while t < tend (its own dt, its own end time);
 // an instance that has arrived stays idle while the others go on.
 //
-// The grid barrier spins with a time limit (EnsArgs::timeout_ns, 2 s): a
-// block that waits longer records an error, every block returns, and the
-// host reports GDF_ERR_TIMEOUT.
+// The grid barrier spins with a time limit (EnsArgs::timeout_ns: 2 s, or
+// 200 ns per cell of the ensemble if longer): a block that waits longer
+// records an error, every block returns, and the host reports
+// GDF_ERR_TIMEOUT.
 
 #include <cuda/atomic>
 #include <cuda_runtime.h>
@@ -608,7 +609,11 @@ int ens_layout(GdfEnsemble* e) {
   A.amax = e->amax;
   A.sync = e->sync;
   A.net = e->net;
-  A.timeout_ns = 2000000000ull;
+  // a phase of a large ensemble may legitimately run for a while: 2 s, or
+  // 200 ns per cell of the whole ensemble if that is longer
+  unsigned long long cells = 0;
+  for (const auto& b : e->in) cells += (unsigned long long)b.K.nx * b.K.ny;
+  A.timeout_ns = std::max(2000000000ull, 200ull * cells);
   A.n = n;
   A.any_faceb = e->any_faceb;
   A.t_lo = e->t_lo;
