@@ -161,6 +161,15 @@ __device__ bool ens_barrier(const EnsArgs& A, int* s_ok) {
   return *s_ok != 0;
 }
 
+// Self-test of the bounded grid barrier: every block but `skip` arrives at
+// one barrier; with skip >= 0 the others wait out the limit and record the
+// error (nothing else is done, so the device stays usable).
+__global__ void __launch_bounds__(ENS_BS) k_barrier_selftest(const __grid_constant__ EnsArgs A, int skip) {
+  __shared__ int s_ok;
+  if ((int)blockIdx.x == skip) return;
+  ens_barrier(A, &s_ok);
+}
+
 __device__ __forceinline__ int tile_instance(const int* off, int n, int t) {
   int lo = 0, hi = n;   // off[lo] <= t < off[hi]
   while (hi - lo > 1) {
@@ -1103,5 +1112,34 @@ int gdf_ens_tune(GdfEnsemble* e, int32_t steps, float* ms_out) {
 }
 
 int64_t gdf_ens_kernel_launches(GdfEnsemble* e) { return e ? e->launches : -1; }
+
+// Runs k_barrier_selftest on `blocks` co-resident blocks with the barrier's
+// time limit set to limit_ns: *timed_out receives 1 when some block gave up
+// waiting (expected when skip_block names one of them), else 0.
+int gdf_ens_barrier_selftest(int32_t blocks, int32_t skip_block, uint64_t limit_ns, int32_t* timed_out) {
+  if (blocks < 1 || blocks > 1024 || !timed_out || limit_ns == 0) return efail(GDF_ERR_ARG, "bad argument");
+  EnsSync* sy = nullptr;
+  ECK(cudaMalloc((void**)&sy, sizeof(EnsSync)));
+  ECK(cudaMemset(sy, 0, sizeof(EnsSync)));
+  EnsArgs A{};
+  A.sync = sy;
+  A.timeout_ns = limit_ns;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)blocks);
+  cfg.blockDim = dim3(ENS_BS);
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaError_t err = cudaLaunchKernelEx(&cfg, k_barrier_selftest, A, (int)skip_block);
+  if (err == cudaSuccess) err = cudaDeviceSynchronize();
+  EnsSync h{};
+  if (err == cudaSuccess) err = cudaMemcpy(&h, sy, sizeof(EnsSync), cudaMemcpyDeviceToHost);
+  cudaFree(sy);
+  if (err != cudaSuccess) return efail(GDF_ERR_CUDA, std::string("barrier self-test: ") + cudaGetErrorString(err));
+  *timed_out = h.err ? 1 : 0;
+  return GDF_OK;
+}
 
 }  // extern "C"

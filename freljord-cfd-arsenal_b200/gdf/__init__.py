@@ -124,6 +124,7 @@ def load(exact: bool = True):
     L.gdf_ens_set_mode.argtypes = [vp, i32]
     L.gdf_ens_tune.argtypes = [vp, i32, C.POINTER(C.c_float)]
     L.gdf_ens_kernel_launches.argtypes = [vp]
+    L.gdf_ens_barrier_selftest.argtypes = [i32, i32, C.c_uint64, ip]
     L.gdf_ens_kernel_launches.restype = C.c_int64
     L.gdf_ens_last_error.restype = C.c_char_p
     _libs[path] = L
@@ -514,3 +515,13 @@ def ensemble_configs(n: int = 64, seed: int = 0, detector: int = DETECT_LEARNED)
             params = blast_params(10_000 + 97 * seed + s)
         out.append((cfg, prob, params, tend))
     return out
+
+
+def ens_barrier_selftest(blocks: int, skip_block: int, limit_ns: int, exact: bool = True) -> bool:
+    """gdf_ens_barrier_selftest: True when the bounded barrier timed out."""
+    L = load(exact)
+    out = C.c_int32()
+    rc = L.gdf_ens_barrier_selftest(blocks, skip_block, limit_ns, C.byref(out))
+    if rc:
+        raise GdfError(rc, L.gdf_ens_last_error().decode())
+    return bool(out.value)

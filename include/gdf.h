@@ -266,6 +266,12 @@ int gdf_ens_get_tiles(GdfEnsemble *e, int32_t *ctas_per_sm, int32_t *face_per_th
 enum { GDF_ENS_TUNE_CANDIDATES = 45 };
 int gdf_ens_tune(GdfEnsemble *e, int32_t steps, float *ms_out);
 int64_t gdf_ens_kernel_launches(GdfEnsemble *e);
+/* Self-test of the persistent mode's bounded grid barrier (no counterpart in
+ * the reference): `blocks` cooperative blocks meet at one barrier whose wait
+ * is limited to limit_ns; skip_block (or -1) names a block that never
+ * arrives. *timed_out = 1 when the others gave up and reported it, 0 when
+ * all met. No state is touched; the device stays usable either way. */
+int gdf_ens_barrier_selftest(int32_t blocks, int32_t skip_block, uint64_t limit_ns, int32_t *timed_out);
 const char *gdf_ens_last_error(void);
 
 /* Lh (as gdf_lh) on caller-owned DEVICE buffers, allocating no device

@@ -149,3 +149,21 @@ def test_ensemble_errors():
     cfg.nx = 1
     with pytest.raises(gdf.GdfError):
         gdf.Ensemble([insts[1][0], cfg])
+
+
+def test_bounded_barrier_reports_a_missing_block_and_device_stays_usable():
+    """The persistent mode's grid barrier waits with a time limit: a block
+    that never arrives (a flag nothing sets) makes the others give up after
+    the limit and report it; nothing faults, and the device keeps working."""
+    import time
+    assert gdf.ens_barrier_selftest(16, -1, 2_000_000_000) is False
+    t0 = time.time()
+    assert gdf.ens_barrier_selftest(16, 5, 50_000_000) is True
+    assert time.time() - t0 < 30
+    insts = mixed_instances()[:2]
+    e = make_ensemble(insts)
+    e.set_mode(0)
+    e.advance(2)
+    for i, (cfg, prob, params, tend) in enumerate(insts):
+        ref, _ = run_single(cfg, prob, params, tend, 2)
+        assert same(e.download(i), ref)
