@@ -1150,9 +1150,11 @@ __device__ __forceinline__ void dt_advance(const Consts& K, double ax, double ay
   sc->steps += 1;
 }
 
-// Fills this module's c_basis on the current device once (the tables do not
-// depend on the configuration). Returns a cudaError_t.
-static inline cudaError_t upload_basis_once(const Consts& K) {
+// Fills this module's c_basis on the current device (the tables do not
+// depend on the configuration). always: on every call (handle creation:
+// survives a reset of the device between handles); otherwise once per
+// device and process. Returns a cudaError_t.
+static inline cudaError_t upload_basis_once(const Consts& K, bool always = false) {
   static std::mutex mu;
   static bool done[256] = {false};
   int dev = 0;
@@ -1160,7 +1162,7 @@ static inline cudaError_t upload_basis_once(const Consts& K) {
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= 256) return cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> lk(mu);
-  if (done[dev]) return cudaSuccess;
+  if (done[dev] && !always) return cudaSuccess;
   Basis B;
   basis_of(K, B);
   e = cudaMemcpyToSymbol(c_basis, &B, sizeof(Basis));

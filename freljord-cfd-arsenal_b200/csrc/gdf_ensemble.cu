@@ -841,7 +841,7 @@ int gdf_ens_create(const GdfConfig* cfgs, int32_t n, GdfEnsemble** out) {
     InstBufs& b = e->in[i];
     b.cfg = cfgs[i];
     consts_for(cfgs[i], b.K);
-    if (i == 0) ok = ok && upload_basis_once(b.K) == cudaSuccess;
+    if (i == 0) ok = ok && upload_basis_once(b.K, true) == cudaSuccess;
     if (b.K.faceb) e->any_faceb = 1;
     const Consts& K = b.K;
     const GdfConfig& c = cfgs[i];

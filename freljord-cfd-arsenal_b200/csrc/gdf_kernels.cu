@@ -715,7 +715,7 @@ int gdf_create(const GdfConfig* cfg, GdfHandle** out) {
   GdfHandle* h = new GdfHandle();
   h->cfg = *cfg;
   build_consts(*cfg, h->K);
-  if (upload_basis_once(h->K) != cudaSuccess) {
+  if (upload_basis_once(h->K, true) != cudaSuccess) {
     cudaGetLastError();
     delete h;
     return fail(GDF_ERR_CUDA, "uploading the basis tables failed");
