@@ -56,17 +56,21 @@ def _run(cmd: list[str]) -> None:
         raise RuntimeError("build failed: " + " ".join(cmd[:3]) + " ...")
 
 
-def build(verbose: bool = False) -> dict:
+def build(verbose: bool = False, jobs: int | None = None) -> dict:
+    """Compile what is stale; the CUDA objects of both libraries compile
+    concurrently (`jobs` at a time, default: the host's cores, at most 6)."""
+    from concurrent.futures import ThreadPoolExecutor
     os.makedirs(LIB, exist_ok=True)
     os.makedirs(BUILD, exist_ok=True)
     nvcc = _nvcc()
     host_o = os.path.join(BUILD, "gdf_host.o")
     io_o = os.path.join(BUILD, "gdf_io.o")
+    cmds = []
     for src, obj in ((HOST_SRC, host_o), (IO_SRC, io_o)):
         if _stale(obj, [src] + HEADERS):
-            _run([HOST_CXX, "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-march=x86-64", "-fopenmp",
-                  "-c", src, "-o", obj])
-    out = {}
+            cmds.append([HOST_CXX, "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-march=x86-64", "-fopenmp",
+                         "-c", src, "-o", obj])
+    libs = []
     for name, flags in (("libgdf_b200.so", ["--fmad=false", "-DGDF_EXACT=1"]),
                         ("libgdf_b200_fma.so", ["--fmad=true"])):
         objs = []
@@ -77,8 +81,16 @@ def build(verbose: bool = False) -> dict:
                        "-Xcompiler", "-fPIC,-ffp-contract=off", "-c", src, "-o", obj]
                 if verbose:
                     cmd.insert(1, "-Xptxas=-v")
-                _run(cmd)
+                cmds.append(cmd)
             objs.append(obj)
+        libs.append((name, objs))
+    if cmds:
+        n = jobs or max(1, min(6, os.cpu_count() or 1))
+        with ThreadPoolExecutor(max_workers=n) as ex:
+            for f in [ex.submit(_run, c) for c in cmds]:
+                f.result()
+    out = {}
+    for name, objs in libs:
         so = os.path.join(LIB, name)
         if _stale(so, objs + [host_o, io_o]):
             _run([nvcc, *ARCH, "-shared", "-o", so, *objs, host_o, io_o, "-Xcompiler", "-fopenmp", "-lgomp"])
