@@ -2,7 +2,8 @@
 """Benchmark of the B200 GDF P2 MHD step: P2 MHD cell-updates/s.
 
 Workload: the MHD rotor at 512x512, P2 modal DG in FP64, HLLD flux, KXRCF
-detector + characteristic TVB limiter + positivity limiter, SSP-RK3 (the
+detector + characteristic TVB limiter with the face-B minmod + positivity
+limiter, SSP-RK3 (the
 plain method at scale). One step = one full SSP-RK3 step of the whole
 grid (3 stages + limiters + div-free reconstruction + dt); one
 cell-update = one cell advanced by one step.
@@ -32,8 +33,8 @@ METRIC = "P2 MHD cell-updates/s on 1 B200, learned-indicator vs plain at equal L
 UNIT = "cell-updates/s"
 NX = NY = 512
 WORKLOAD = ("MHD rotor 512x512 on [0,1]^2, P2 modal DG FP64 (8 vars x 10 modal slots), HLLD flux, "
-            "KXRCF detector + characteristic TVB (M=10) + positivity limiter, corner-Ez CT + Balsara "
-            "div-free B, SSP-RK3, CFL 0.15 (plain method)")
+            "KXRCF detector + characteristic TVB (M=10) + face-B minmod + positivity limiter, corner-Ez "
+            "CT + Balsara div-free B, SSP-RK3, CFL 0.15 (plain method)")
 
 # Compulsory HBM bytes per cell for one launch of each kernel kind (FP64,
 # 52 live modal slots = 416 B per cell state): what one launch must read
@@ -44,10 +45,15 @@ ALG_BYTES_PER_CELL = {
     "vertex": 416 + 8,                       # cell modes once, one vertex Ez
     "cell": (1888 + 2 * 2304) / 3,           # U + faces' Fhat + U0/UI read, UI (+U0) written; stage mean
     "bface": 2 * (5 * 8 + 8 + 3 * 8 * 3),    # two faces: Ez points, vertex, B/B0/BI read+written
-    "limit": 416 + 2 * 6 * 8 + 416 + 4,      # pre-limit modes, 4 face polys (2 owned), limited modes, flag
+    "limit": 416 + 416 + 4,                  # pre-limit modes, limited modes, flag (face-B minmod on:
+                                             # the div-free reconstruction is its own kernel)
+    "faceb_limit": 8 * 8 + 2 * 4 * 8,        # 4 Bx + 4 By modes of the cell, 2 coefficients of its 2 faces r+w
+    "divfree": 2 * 3 * 8 + 16 * 8,           # 3 coefficients of 2 owned faces, 16 B modes written
     "set_bc": 0.0,
     "dt": 8 * 8,                             # cell averages
 }
+# the limiter with the div-free reconstruction fused (face-B minmod off)
+ALG_BYTES_LIMIT_FUSED = 416 + 2 * 6 * 8 + 416 + 4   # + 4 face polys (2 owned)
 
 
 def read_peaks():
@@ -60,61 +66,111 @@ def read_peaks():
         return 6650.0, "fallback"
 
 
+def nvml_index(local: int):
+    """NVML handle of this process's CUDA device: NVML numbers GPUs
+    regardless of CUDA_VISIBLE_DEVICES, so follow its entry (an index or a
+    GPU UUID) when it is set."""
+    import pynvml
+    vis = [v.strip() for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
+    if local < len(vis):
+        v = vis[local]
+        if v.startswith("GPU-"):
+            return pynvml.nvmlDeviceGetHandleByUUID(v)
+        if v.isdigit():
+            return pynvml.nvmlDeviceGetHandleByIndex(int(v))
+    return pynvml.nvmlDeviceGetHandleByIndex(local)
+
+
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clock and clock-event (throttle) reasons sampled through NVML every
+    10 ms on a thread, each sample stamped; `mark()` brackets the timed
+    region and only samples inside it count. Reading only: nothing is set.
+    Falls back to `nvidia-smi -lms 100` when NVML is not importable."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4), ("hw_power_brake_slowdown", 0x80))
 
     def __init__(self, device: int):
         self.device = device
         self.proc = None
-        self.lines: list[str] = []
         self.t = None
+        self.stop_evt = threading.Event()
+        self.samples: list[tuple] = []     # (time, sm MHz, max MHz, reasons bitmask)
+        self.window = None
+        self.source = None
 
     def start(self):
         try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = nvml_index(self.device)
+            smax = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+
+            def poll():
+                while not self.stop_evt.is_set():
+                    try:
+                        sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                        r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        self.samples.append((time.perf_counter(), float(sm), float(smax), int(r)))
+                    except Exception:
+                        pass
+                    time.sleep(0.01)
+            self.source = "nvml"
+            self.t = threading.Thread(target=poll, daemon=True)
+            self.t.start()
+            return
+        except Exception:
+            pass
+        try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
+            self.source = "nvidia-smi"
+            self.t = threading.Thread(target=self._read_smi, daemon=True)
             self.t.start()
         except Exception:
             self.proc = None
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
-    def stop(self) -> dict | None:
-        if not self.proc:
-            return None
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        if self.t:
-            self.t.join(timeout=2)
-        sm, smax, reasons = [], [], set()
-        names = ["active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+    def _read_smi(self):
+        bits = dict(self.REASONS)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.proc.stdout:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
             try:
-                sm.append(float(f[1]))
-                smax.append(float(f[2]))
+                r = sum(bits[nm] for nm, v in zip(names, f[5:9]) if v.lower() == "active")
+                self.samples.append((time.perf_counter(), float(f[1]), float(f[2]), r))
             except ValueError:
                 continue
-            for nm, v in zip(names[1:], f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        if not sm:
+
+    def mark(self, t0: float, t1: float):
+        """The host times that bracket the timed region."""
+        self.window = (t0, t1)
+
+    def stop(self) -> dict | None:
+        self.stop_evt.set()
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if self.t:
+            self.t.join(timeout=2)
+        if not self.samples:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
-                "samples": len(sm)}
+        inside = self.samples
+        if self.window:
+            t0, t1 = self.window
+            inside = [x for x in self.samples if t0 <= x[0] <= t1] or \
+                [min(self.samples, key=lambda x: abs(x[0] - 0.5 * (t0 + t1)))]
+        reasons = sorted({nm for _, _, _, r in inside for nm, b in self.REASONS if r & b})
+        return {"sm_mhz": statistics.median(x[1] for x in inside), "sm_max_mhz": max(x[2] for x in inside),
+                "reasons": reasons, "samples": len(inside), "source": self.source}
 
 
 def dist_env():
@@ -393,9 +449,11 @@ def run_ours(args):
         dist.barrier()
     clk = ClockSampler(local)
     clk.start()
-    time.sleep(0.3)
+    time.sleep(0.05)
     l0 = s.kernel_launches()
-    _, taken, ms = s.advance_timed(1e9, args.steps)
+    h0 = time.perf_counter()
+    _, taken, ms = s.advance_timed(1e9, args.steps)   # returns after the device finished
+    clk.mark(h0, time.perf_counter())
     launches = s.kernel_launches() - l0
     clocks = clk.stop()
     ms_max = reduce_max_ms(ms, dist, f"cuda:{local}")
@@ -405,7 +463,8 @@ def run_ours(args):
     prof = s.profile(2)
     dom = max((k for k in prof if k in ALG_BYTES_PER_CELL), key=lambda k: prof[k][0] * prof[k][1])
     dom_ms, dom_per_step = prof[dom]
-    alg_bytes = ALG_BYTES_PER_CELL[dom] * NX * NY
+    per_cell = ALG_BYTES_LIMIT_FUSED if dom == "limit" and not cfg.faceb_limiter else ALG_BYTES_PER_CELL[dom]
+    alg_bytes = per_cell * NX * NY
     peak, peak_kind = read_peaks()
     achieved = alg_bytes / (dom_ms / 1e3) / 1e9
     traffic = None
@@ -503,7 +562,7 @@ def run_ours(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -176,6 +176,9 @@ int gdf_problem_config(int32_t problem, int32_t nx, int32_t ny, GdfConfig* out, 
       out->pp_limiter = 1;
       out->detector = GDF_DETECT_KXRCF;
       out->kxrcf_ck = 1.0;
+      // the face-B minmod as for the blast: with the raw face B the rotor
+      // loses positivity near t = 0.013 (step 27 at 64^2, 55 at 128^2)
+      out->faceb_limiter = 1;
       te = 0.295;
       break;
     case GDF_PROB_BLAST:

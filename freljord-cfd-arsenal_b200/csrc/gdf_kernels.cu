@@ -563,10 +563,10 @@ static int launch_limit(GdfHandle* h, const double* S, double* D, int stage, con
     // face-B minmod, div-free reconstruction
     int rc = launch_set_bc(h, D, 0, sc_gate);
     if (rc) return rc;
-    rc = run_kernel(h, GDF_K_LIMIT, [&] {
+    rc = run_kernel(h, GDF_K_FACEB_LIMIT, [&] {
       k_faceb_limit<<<nblk(K.fxplane + K.fyplane, 128), 128, 0, h->st>>>(K, D, h->BX, h->BY, sc_gate);
     });
-    if (!rc) rc = run_kernel(h, GDF_K_LIMIT, [&] { k_divfree<<<nblk(ncell, 128), 128, 0, h->st>>>(K, D, h->BX, h->BY, sc_gate); });
+    if (!rc) rc = run_kernel(h, GDF_K_DIVFREE, [&] { k_divfree<<<nblk(ncell, 128), 128, 0, h->st>>>(K, D, h->BX, h->BY, sc_gate); });
     if (rc) return rc;
   }
   return GDF_OK;

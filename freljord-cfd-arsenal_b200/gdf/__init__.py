@@ -33,7 +33,8 @@ ENS_TUNE_CANDIDATES = 45
 MLP_NPARAM = 10049
 NFEAT = 90
 
-KERNEL_NAMES = ["set_bc", "face_x", "face_y", "vertex", "cell", "bface", "limit", "dt", "diag"]
+KERNEL_NAMES = ["set_bc", "face_x", "face_y", "vertex", "cell", "bface", "limit", "dt", "diag", "faceb_limit",
+                "divfree"]
 KERNEL_KINDS = len(KERNEL_NAMES)
 
 LIB_EXACT = os.path.join(LIB_DIR, "libgdf_b200.so")

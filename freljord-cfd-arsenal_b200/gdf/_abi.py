@@ -103,7 +103,7 @@ def problem_config(problem: int, nx: int, ny: int) -> tuple[GdfConfig, float]:
         c.xa, c.xb, c.ya, c.yb = 0.0, 2 * pi, 0.0, 2 * pi
         c.tvb_m = 50.0
         tend = 0.5
-    elif problem == PROB_ROTOR:           # rotor: HLLD, gamma 1.4, KXRCF + pp
+    elif problem == PROB_ROTOR:           # rotor: HLLD, gamma 1.4, KXRCF + pp, face-B minmod
         c.xa, c.xb, c.ya, c.yb = 0.0, 1.0, 0.0, 1.0
         c.gamma = 1.4
         c.flux_type = FLUX_HLLD
@@ -111,6 +111,7 @@ def problem_config(problem: int, nx: int, ny: int) -> tuple[GdfConfig, float]:
         c.detector = DETECT_KXRCF
         c.kxrcf_ck = 1.0
         c.tvb_m = 10.0
+        c.faceb_limiter = 1                # face-B minmod (raw face B loses positivity near t = 0.013)
         tend = 0.295
     elif problem == PROB_BLAST:           # blast: HLLD, gamma 1.4, pp, outflow
         c.xa, c.xb, c.ya, c.yb = -0.5, 0.5, -0.5, 0.5

@@ -312,7 +312,9 @@ void *gdf_stream(GdfHandle *h);
 enum {
   GDF_K_SET_BC = 0, GDF_K_FACE_X = 1, GDF_K_FACE_Y = 2, GDF_K_VERTEX = 3,
   GDF_K_CELL = 4, GDF_K_BFACE = 5, GDF_K_LIMIT = 6, GDF_K_DT = 7, GDF_K_DIAG = 8,
-  GDF_KERNEL_KINDS = 9
+  GDF_K_FACEB_LIMIT = 9, /* face-B minmod (faceb_limiter) */
+  GDF_K_DIVFREE = 10,    /* div-free reconstruction when not fused into the limiter */
+  GDF_KERNEL_KINDS = 11
 };
 
 /* Run `steps` time steps of the resident state with CUDA events around

@@ -23,7 +23,7 @@ from oracle import Oracle  # noqa: E402
 # name: (problem, nx, ny, config edits, steps)
 CASES = {
     "ot_hll_all_10x8": (gdf.PROB_ORSZAG_TANG, 10, 8, {}, 3),
-    "rotor_hlld_kxrcf_pp_12x12": (gdf.PROB_ROTOR, 12, 12, {}, 3),
+    "rotor_hlld_kxrcf_pp_12x12": (gdf.PROB_ROTOR, 12, 12, {"faceb_limiter": 0}, 3),   # raw face B
     "blast_hlld_faceb_10x12": (gdf.PROB_BLAST, 10, 12, {}, 3),
     "cloud_hllc_12x6": (gdf.PROB_CLOUD_SHOCK, 12, 6, {"flux_type": gdf.FLUX_HLLC}, 2),
     "vortex_lf_8x8": (gdf.PROB_VORTEX, 8, 8, {"flux_type": gdf.FLUX_LF}, 2),

@@ -27,6 +27,7 @@ TOL_FMA_STEP = 1e-8  # FMA build, whole step (threshold decisions may flip)
 CASES = {
     "ot": (gdf.PROB_ORSZAG_TANG, 24, 16),
     "rotor": (gdf.PROB_ROTOR, 20, 20),
+    "rotor_raw_faceb": (gdf.PROB_ROTOR, 20, 20, {"faceb_limiter": 0}),
     "blast": (gdf.PROB_BLAST, 16, 18),
     "cloud": (gdf.PROB_CLOUD_SHOCK, 24, 12),
     "vortex": (gdf.PROB_VORTEX, 16, 16),
@@ -34,8 +35,10 @@ CASES = {
 
 
 def setup(case, edit=None):
-    problem, nx, ny = CASES[case]
+    problem, nx, ny, *edits = CASES[case]
     cfg, _ = gdf.problem_config(problem, nx, ny)
+    for k, v in (edits[0] if edits else {}).items():
+        setattr(cfg, k, v)
     if edit:
         edit(cfg)
     o = Oracle(cfg)
