@@ -157,3 +157,17 @@ def test_download_live_writes_only_live_planes():
     assert np.array_equal(marked[live], full[0][live])
     assert np.all(marked[~live] == 7.0)
     assert np.array_equal(b1, full[1]) and np.array_equal(b2, full[2])
+
+
+@pytest.mark.gpu
+def test_driver_checkpoint_restart_continues_value_exact(tmp_path):
+    from gdf.run import run
+    full, part = str(tmp_path / "full"), str(tmp_path / "part")
+    ckpt = str(tmp_path / "r.ckpt")
+    t5, n5, _ = run(gdf.PROB_ROTOR, 24, 20, full, tend=1.0, max_steps=5)
+    t3, n3, L2 = run(gdf.PROB_ROTOR, 24, 20, part, tend=1.0, max_steps=3, checkpoint=ckpt, save=False)
+    assert (n5, n3) == (5, 3) and L2 is None and not os.path.exists(os.path.join(part, "Q1.txt"))
+    t, n, _ = run(gdf.PROB_ROTOR, 24, 20, part, tend=1.0, max_steps=2, restart=ckpt)
+    assert n == 2 and t == t5 and t3 < t5
+    for q in ("Q1.txt", "Q6.txt", "Q7.txt"):
+        assert np.array_equal(np.loadtxt(os.path.join(full, q)), np.loadtxt(os.path.join(part, q)))
