@@ -997,13 +997,35 @@ __device__ __forceinline__ void lim_finish(const Consts& K, double* __restrict__
   if (!(m[0][0] > 0.0) || !isfinite(m[4][0])) atomicOr(&sc->status, 1);
 }
 
-template <int LM>
+// Appends the gated cells among the calling warp's active lanes to list
+// (one atomic per warp); true for a gated cell.
+__device__ __forceinline__ bool lim_defer(bool gate, long long item, int32_t* __restrict__ list,
+                                          int32_t* __restrict__ count) {
+  const unsigned act = __activemask();
+  const unsigned bal = __ballot_sync(act, gate);
+  if (!gate) return false;
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(bal) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(count, __popc(bal));
+  base = __shfl_sync(bal, base, leader);
+  list[base + __popc(bal & ((1u << lane) - 1u))] = (int32_t)item;
+  return true;
+}
+
+// One interior cell of the limiter. COMPACT: a gated cell is only appended
+// to list (limit_tvb_item finishes it in a second pass over full warps, so
+// the characteristic limiter never runs beside idle lanes); an ungated one
+// is finished here.
+template <int LM, bool COMPACT = false>
 __device__ __forceinline__ void limit_item(const Consts& K, const double* __restrict__ S, double* __restrict__ D,
                                            const double* __restrict__ BX, const double* __restrict__ BY,
                                            int32_t* __restrict__ flags, int32_t* __restrict__ trouble, int stage,
                                            int divfree, Scal* __restrict__ sc, const MlpDev* __restrict__ net,
                                            const float* __restrict__ QM, float* __restrict__ pnet,
-                                           float t_lo, float t_hi, long long item, unsigned char* lsm) {
+                                           float t_lo, float t_hi, long long item, unsigned char* lsm,
+                                           int32_t* __restrict__ list = nullptr,
+                                           int32_t* __restrict__ count = nullptr) {
   const bool valid = item < (long long)K.nx * K.ny;
   const int i = valid ? (int)(item % K.nx) + 1 : 1;
   const int j = valid ? (int)(item / K.nx) + 1 : 1;
@@ -1012,7 +1034,32 @@ __device__ __forceinline__ void limit_item(const Consts& K, const double* __rest
   int32_t word = 0;
   const bool gate = lim_gate<LM>(K, S, trouble, net, QM, pnet, t_lo, t_hi, item, lsm, valid, c, m, word);
   if (!valid) return;
-  if (gate) lim_tvb(K, S, c, m, word);
+  if (COMPACT) {
+    if (lim_defer(gate, item, list, count)) return;
+  } else if (gate) {
+    lim_tvb(K, S, c, m, word);
+  }
+  lim_finish(K, D, BX, BY, flags, stage, divfree, sc, item, i, j, c, m, word);
+}
+
+// The second pass for a cell limit_item<LM, true> deferred: its pre-limit
+// modes again, the detector bit lim_gate set for it (any detector but
+// GDF_DETECT_ALL), the characteristic limiter and the finish.
+__device__ __forceinline__ void limit_tvb_item(const Consts& K, const double* __restrict__ S, double* __restrict__ D,
+                                               const double* __restrict__ BX, const double* __restrict__ BY,
+                                               int32_t* __restrict__ flags, int stage, int divfree,
+                                               Scal* __restrict__ sc, long long item) {
+  const long long pl = K.plane;
+  const int i = (int)(item % K.nx) + 1;
+  const int j = (int)(item / K.nx) + 1;
+  const long long c = i + (long long)K.nx2 * j;
+  double m[NE][NP];
+#pragma unroll
+  for (int n = 0; n < NE; ++n)
+#pragma unroll
+    for (int d = 0; d < NP; ++d) m[n][d] = live_mode(n, d) ? S[c + pl * (d + 10 * n)] : 0.0;
+  int32_t word = K.detector != GDF_DETECT_ALL ? (1 << 24) : 0;
+  lim_tvb(K, S, c, m, word);
   lim_finish(K, D, BX, BY, flags, stage, divfree, sc, item, i, j, c, m, word);
 }
 

@@ -123,17 +123,34 @@ __global__ void k_features(const __grid_constant__ Consts K, const float* __rest
   for (int k = 0; k < NFEAT; ++k) X[item * NFEAT + k] = f[k];
 }
 
-template <int LM>
+template <int LM, bool COMPACT>
 __global__ void __launch_bounds__(LIM_BS, GDF_LIMIT_MINB) k_limit(const __grid_constant__ Consts K, const double* __restrict__ S,
                                                   double* __restrict__ D, const double* __restrict__ BX,
                                                   const double* __restrict__ BY, int32_t* __restrict__ flags,
                                                   int32_t* __restrict__ trouble, int stage, int divfree,
                                                   const Scal* __restrict__ gate_sc, Scal* __restrict__ sc,
                                                   const MlpDev* __restrict__ net, const float* __restrict__ QM,
-                                                  float* __restrict__ pnet, float t_lo, float t_hi) {
+                                                  float* __restrict__ pnet, float t_lo, float t_hi,
+                                                  int32_t* __restrict__ list, int32_t* __restrict__ count) {
   extern __shared__ __align__(16) unsigned char lsm[];
   if (gate_sc && !gate_sc->active) return;
-  limit_item<LM>(K, S, D, BX, BY, flags, trouble, stage, divfree, sc, net, QM, pnet, t_lo, t_hi, gtid(), lsm);
+  limit_item<LM, COMPACT>(K, S, D, BX, BY, flags, trouble, stage, divfree, sc, net, QM, pnet, t_lo, t_hi, gtid(), lsm,
+                          list, count);
+}
+
+// The cells k_limit<LM, true> deferred, one per thread (the grid covers
+// every interior cell; threads past the count return).
+__global__ void __launch_bounds__(LIM_BS, GDF_LIMIT_MINB) k_limit_tvb(const __grid_constant__ Consts K,
+                                                  const double* __restrict__ S, double* __restrict__ D,
+                                                  const double* __restrict__ BX, const double* __restrict__ BY,
+                                                  int32_t* __restrict__ flags, int stage, int divfree,
+                                                  const Scal* __restrict__ gate_sc, Scal* __restrict__ sc,
+                                                  const int32_t* __restrict__ list,
+                                                  const int32_t* __restrict__ count) {
+  if (gate_sc && !gate_sc->active) return;
+  const long long t = gtid();
+  if (t >= *count) return;
+  limit_tvb_item(K, S, D, BX, BY, flags, stage, divfree, sc, list[t]);
 }
 
 __global__ void k_faceb_limit(const __grid_constant__ Consts K, const double* __restrict__ S,
@@ -310,6 +327,7 @@ struct GdfHandle {
   MlpDev* net = nullptr;     // learned-indicator network (device copy)
   float t_lo = 0.5f, t_hi = 0.5f;
   int32_t *flags = nullptr, *trouble = nullptr;
+  int32_t *lim_list = nullptr, *lim_count = nullptr;  // cells the limiter's first pass deferred
   Scal* sc = nullptr;
   Scal* sc_host = nullptr;  // pinned mirror
   int uploaded = 0;
@@ -543,21 +561,37 @@ static int launch_limit(GdfHandle* h, const double* S, double* D, int stage, con
       smem = LIMIT_SMEM_LEARNED;
     }
   }
+  // with a detector, gated cells go to a second pass over full warps
+  const bool compact = K.detector != GDF_DETECT_ALL;
+  if (compact) CK(cudaMemsetAsync(h->lim_count, 0, sizeof(int32_t), h->st));
+  int32_t *L = h->lim_list, *N = h->lim_count;
   int rc0 = run_kernel(h, GDF_K_LIMIT, [&] {
     const unsigned nb = nblk(ncell, LIM_BS);
     if (K.detector == GDF_DETECT_LEARNED && infer)
-      k_limit<LIM_INFER><<<nb, LIM_BS, smem, h->st>>>(K, S, D, h->BX, h->BY, h->flags, h->trouble, stage,
-                                                      fused_divfree, sc_gate, h->sc, h->net, h->QM, h->pnet, h->t_lo,
-                                                      h->t_hi);
+      k_limit<LIM_INFER, true><<<nb, LIM_BS, smem, h->st>>>(K, S, D, h->BX, h->BY, h->flags, h->trouble, stage,
+                                                            fused_divfree, sc_gate, h->sc, h->net, h->QM, h->pnet,
+                                                            h->t_lo, h->t_hi, L, N);
     else if (K.detector == GDF_DETECT_LEARNED)
-      k_limit<LIM_PNET><<<nb, LIM_BS, 0, h->st>>>(K, S, D, h->BX, h->BY, h->flags, h->trouble, stage, fused_divfree,
-                                                  sc_gate, h->sc, h->net, h->QM, h->pnet, h->t_lo, h->t_hi);
+      k_limit<LIM_PNET, true><<<nb, LIM_BS, 0, h->st>>>(K, S, D, h->BX, h->BY, h->flags, h->trouble, stage,
+                                                        fused_divfree, sc_gate, h->sc, h->net, h->QM, h->pnet,
+                                                        h->t_lo, h->t_hi, L, N);
+    else if (compact)
+      k_limit<LIM_PLAIN, true><<<nb, LIM_BS, 0, h->st>>>(K, S, D, h->BX, h->BY, h->flags, h->trouble, stage,
+                                                         fused_divfree, sc_gate, h->sc, nullptr, nullptr, nullptr,
+                                                         0.f, 0.f, L, N);
     else
-      k_limit<LIM_PLAIN><<<nb, LIM_BS, 0, h->st>>>(K, S, D, h->BX, h->BY, h->flags, h->trouble, stage,
-                                                   fused_divfree, sc_gate, h->sc, nullptr, nullptr, nullptr, 0.f,
-                                                   0.f);
+      k_limit<LIM_PLAIN, false><<<nb, LIM_BS, 0, h->st>>>(K, S, D, h->BX, h->BY, h->flags, h->trouble, stage,
+                                                          fused_divfree, sc_gate, h->sc, nullptr, nullptr, nullptr,
+                                                          0.f, 0.f, nullptr, nullptr);
   });
   if (rc0) return rc0;
+  if (compact) {
+    rc0 = run_kernel(h, GDF_K_LIMIT_TVB, [&] {
+      k_limit_tvb<<<nblk(ncell, LIM_BS), LIM_BS, 0, h->st>>>(K, S, D, h->BX, h->BY, h->flags, stage, fused_divfree,
+                                                             sc_gate, h->sc, L, N);
+    });
+    if (rc0) return rc0;
+  }
   if (K.faceb) {
     // TVB_Limiter_P2.f90:126-187 then div_free: set_bc on the limited state,
     // face-B minmod, div-free reconstruction
@@ -742,6 +776,8 @@ int gdf_create(const GdfConfig* cfg, GdfHandle** out) {
   ok = ok && alloc((void**)&h->part, (size_t)(h->dt_blocks + 1) * 4 * sizeof(double));
   ok = ok && alloc((void**)&h->flags, (size_t)ncell * sizeof(int32_t)) &&
        alloc((void**)&h->trouble, (size_t)ncell * sizeof(int32_t));
+  ok = ok && alloc((void**)&h->lim_list, (size_t)ncell * sizeof(int32_t)) &&
+       alloc((void**)&h->lim_count, sizeof(int32_t));
   ok = ok && alloc((void**)&h->sc, sizeof(Scal));
   ok = ok && cudaMallocHost((void**)&h->sc_host, sizeof(Scal)) == cudaSuccess;
   if (!ok) {
@@ -775,6 +811,8 @@ int gdf_destroy(GdfHandle* h) {
   if (h->net) cudaFree(h->net);
   if (h->flags) cudaFree(h->flags);
   if (h->trouble) cudaFree(h->trouble);
+  if (h->lim_list) cudaFree(h->lim_list);
+  if (h->lim_count) cudaFree(h->lim_count);
   if (h->sc) cudaFree(h->sc);
   if (h->sc_host) cudaFreeHost(h->sc_host);
   if (h->st) cudaStreamDestroy(h->st);

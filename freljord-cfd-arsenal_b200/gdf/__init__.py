@@ -34,7 +34,7 @@ MLP_NPARAM = 10049
 NFEAT = 90
 
 KERNEL_NAMES = ["set_bc", "face_x", "face_y", "vertex", "cell", "bface", "limit", "dt", "diag", "faceb_limit",
-                "divfree"]
+                "divfree", "limit_tvb"]
 KERNEL_KINDS = len(KERNEL_NAMES)
 
 LIB_EXACT = os.path.join(LIB_DIR, "libgdf_b200.so")

@@ -314,7 +314,8 @@ enum {
   GDF_K_CELL = 4, GDF_K_BFACE = 5, GDF_K_LIMIT = 6, GDF_K_DT = 7, GDF_K_DIAG = 8,
   GDF_K_FACEB_LIMIT = 9, /* face-B minmod (faceb_limiter) */
   GDF_K_DIVFREE = 10,    /* div-free reconstruction when not fused into the limiter */
-  GDF_KERNEL_KINDS = 11
+  GDF_K_LIMIT_TVB = 11,  /* the limiter's second pass over the gated cells */
+  GDF_KERNEL_KINDS = 12
 };
 
 /* Run `steps` time steps of the resident state with CUDA events around
