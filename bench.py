@@ -47,6 +47,7 @@ ALG_BYTES_PER_CELL = {
     "bface": 2 * (5 * 8 + 8 + 3 * 8 * 3),    # two faces: Ez points, vertex, B/B0/BI read+written
     "limit": 416 + 416 + 4,                  # pre-limit modes, limited modes, flag (face-B minmod on:
                                              # the div-free reconstruction is its own kernel)
+    "limit_tvb": 416 + 416 + 4,              # per deferred (gated) cell: modes, limited modes, flag
     "faceb_limit": 8 * 8 + 2 * 4 * 8,        # 4 Bx + 4 By modes of the cell, 2 coefficients of its 2 faces r+w
     "divfree": 2 * 3 * 8 + 16 * 8,           # 3 coefficients of 2 owned faces, 16 B modes written
     "set_bc": 0.0,
@@ -463,8 +464,19 @@ def run_ours(args):
     prof = s.profile(2)
     dom = max((k for k in prof if k in ALG_BYTES_PER_CELL), key=lambda k: prof[k][0] * prof[k][1])
     dom_ms, dom_per_step = prof[dom]
-    per_cell = ALG_BYTES_LIMIT_FUSED if dom == "limit" and not cfg.faceb_limiter else ALG_BYTES_PER_CELL[dom]
-    alg_bytes = per_cell * NX * NY
+    # with a detector the limiter runs in two passes: the first reads every
+    # cell and writes the ungated ones, the second takes the gated cells (the
+    # sticky KXRCF flags)
+    flagged = int((s.trouble() != 0).sum())
+    ncell = NX * NY
+    if dom == "limit_tvb":
+        alg_bytes = ALG_BYTES_PER_CELL["limit_tvb"] * flagged
+    elif dom == "limit":
+        alg_bytes = 416 * ncell + (416 + 4) * (ncell - flagged) + 4 * flagged
+        if not cfg.faceb_limiter:
+            alg_bytes += (ALG_BYTES_LIMIT_FUSED - ALG_BYTES_PER_CELL["limit"]) * (ncell - flagged)
+    else:
+        alg_bytes = ALG_BYTES_PER_CELL[dom] * ncell
     peak, peak_kind = read_peaks()
     achieved = alg_bytes / (dom_ms / 1e3) / 1e9
     traffic = None
@@ -538,7 +550,7 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "alg_bytes_per_launch": alg_bytes, "ms_per_launch": dom_ms,
-                         "launches_per_step": dom_per_step},
+                         "launches_per_step": dom_per_step, "flagged_cells": flagged},
             "kernels_ms_per_launch": {k: v[0] for k, v in prof.items() if v[1]},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d_bytes),
                     "d2h_bytes_per_step": int(h2d_bytes), "steps": e2e_steps,

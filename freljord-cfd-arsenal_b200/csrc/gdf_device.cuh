@@ -1043,8 +1043,9 @@ __device__ __forceinline__ void limit_item(const Consts& K, const double* __rest
 }
 
 // The second pass for a cell limit_item<LM, true> deferred: its pre-limit
-// modes again, the detector bit lim_gate set for it (any detector but
-// GDF_DETECT_ALL), the characteristic limiter and the finish.
+// modes again, the detector bit lim_gate set for it (KXRCF and the learned
+// gate set it; GDF_DETECT_ALL does not), the characteristic limiter and the
+// finish.
 __device__ __forceinline__ void limit_tvb_item(const Consts& K, const double* __restrict__ S, double* __restrict__ D,
                                                const double* __restrict__ BX, const double* __restrict__ BY,
                                                int32_t* __restrict__ flags, int stage, int divfree,
