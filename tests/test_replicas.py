@@ -55,3 +55,38 @@ def test_reference_arm_nonzero_rank_exits_quietly():
 def test_single_rank_reduce_is_identity():
     import bench
     assert bench.reduce_max_ms(3.5, None, "cpu") == 3.5
+
+
+def test_clock_sampler_counts_only_the_timed_window(monkeypatch):
+    """Clock samples outside the host times that bracket the timed region
+    are left out; the clock-event reason bits decode to their names; with no
+    sample inside a short window the nearest one stands in."""
+    import bench
+    c = bench.ClockSampler(0)
+    c.samples = [(1.0, 1100.0, 1965.0, 0x1), (2.0, 1965.0, 1965.0, 0x4), (2.5, 1950.0, 1965.0, 0x4 | 0x40),
+                 (9.0, 900.0, 1965.0, 0x8)]
+    c.mark(1.5, 3.0)
+    r = c.stop()
+    assert r["samples"] == 2 and r["sm_mhz"] == 1957.5 and r["sm_max_mhz"] == 1965.0
+    assert r["reasons"] == ["hw_thermal_slowdown", "sw_power_cap"]
+    c = bench.ClockSampler(0)
+    c.samples = [(1.0, 1000.0, 1965.0, 0), (5.0, 1965.0, 1965.0, 0)]
+    c.mark(4.5, 4.6)
+    r = c.stop()
+    assert r["samples"] == 1 and r["sm_mhz"] == 1965.0 and r["reasons"] == []
+    monkeypatch.setenv("CUDA_VISIBLE_DEVICES", "GPU-1234,3")
+    calls = []
+
+    class FakeNvml:
+        @staticmethod
+        def nvmlDeviceGetHandleByUUID(u):
+            calls.append(("uuid", u))
+
+        @staticmethod
+        def nvmlDeviceGetHandleByIndex(i):
+            calls.append(("index", i))
+    monkeypatch.setitem(sys.modules, "pynvml", FakeNvml)
+    bench.nvml_index(0)
+    bench.nvml_index(1)
+    bench.nvml_index(2)
+    assert calls == [("uuid", "GPU-1234"), ("index", 3), ("index", 2)]
