@@ -1,12 +1,18 @@
 #!/usr/bin/env python
-"""Benchmark of the B200 GDF P2 MHD step: P2 MHD cell-updates/s.
+"""Benchmark of the B200 GDF P2 MHD step: P2 MHD cell-updates/s, the
+learned troubled-cell indicator against the plain method.
 
-Workload: the MHD rotor at 512x512, P2 modal DG in FP64, HLLD flux, KXRCF
-detector + characteristic TVB limiter with the face-B minmod + positivity
-limiter, SSP-RK3 (the
-plain method at scale). One step = one full SSP-RK3 step of the whole
-grid (3 stages + limiters + div-free reconstruction + dt); one
-cell-update = one cell advanced by one step.
+Workload (the largest single-GPU configuration): the strong MHD blast on a
+2048x2048 grid, [-0.5,0.5]^2, gamma 1.4, rho 1, p 1000 inside r < 0.1 and
+0.1 outside, Bx = By = 100/sqrt(8 pi), P2 modal DG in FP64, HLLD flux,
+corner-Ez CT with Balsara's divergence-free B, positivity limiter on,
+SSP-RK3, CFL 0.15. `value` is the learned-indicator method (network gate,
+KXRCF deciding in its uncertain band, characteristic TVB limiter where the
+gate fires); the plain method (sticky KXRCF detector, the reference's)
+runs the same steps beside it. One step = one full SSP-RK3 step of the
+whole grid (3 stages + limiters + div-free reconstruction + dt); one
+cell-update = one cell advanced by one step. The timed steps start from
+t = 0 after `--warmup` untimed steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -14,6 +20,16 @@ N > 1 runs one process per GPU under torchrun; each rank advances its own
 replica of the workload (the path runs on one GPU; replicas only), timed
 on the device and reported as the max over ranks. Prints one JSON line on
 rank 0.
+
+--impl reference times the reference method on the host cores: the CPU
+restatement of the reference (oracle/, compiled without FMA like a
+gfortran build of the Fortran, OpenMP over every host thread) on a bounded
+sample of the same workload, a 2048x256 band of the blast grid (rows
+1152-1407, y in [1/16, 3/16]: same cell size and initial data, outflow at
+the band's own edges), one full SSP-RK3 step of the band per step. The band
+cuts the initial blast disc so that 3.3% of its cells start inside it, as
+3.1% of the whole grid's do, which keeps the sample's mix of limiter-heavy
+and quiet cells close to the whole grid's.
 """
 from __future__ import annotations
 
@@ -31,30 +47,22 @@ sys.path.insert(0, os.path.join(REPO, "freljord-cfd-arsenal_b200"))
 
 METRIC = "P2 MHD cell-updates/s on 1 B200, learned-indicator vs plain at equal L1 err"
 UNIT = "cell-updates/s"
-NX = NY = 512
-WORKLOAD = ("MHD rotor 512x512 on [0,1]^2, P2 modal DG FP64 (8 vars x 10 modal slots), HLLD flux, "
-            "KXRCF detector + characteristic TVB (M=10) + face-B minmod + positivity limiter, corner-Ez "
-            "CT + Balsara div-free B, SSP-RK3, CFL 0.15 (plain method)")
+NX = NY = 2048
+BAND = 256                     # rows of the CPU sample band (of NY)
+WORKLOAD = ("Strong MHD blast 2048x2048 on [-0.5,0.5]^2, P2 modal DG FP64 (8 vars x 10 modal slots), gamma 1.4, "
+            "rho 1, p 1000 (r<0.1) / 0.1, Bx=By=100/sqrt(8pi), HLLD flux, corner-Ez CT + Balsara div-free B, "
+            "positivity limiter + characteristic TVB (M=10) + face-B minmod, SSP-RK3, CFL 0.15; learned "
+            "troubled-cell indicator (KXRCF judge in its band) vs the plain sticky-KXRCF method")
+CONFIG = {"workload": WORKLOAD, "grid": [NX, NY], "problem": "blast", "tend": 0.01,
+          "method": "learned indicator vs plain", "dtype": "f64",
+          "l2": "inputs larger than L2 (one state copy is 1.75 GB of live slots; 126 MB L2)"}
 
-# Compulsory HBM bytes per cell for one launch of each kernel kind (FP64,
-# 52 live modal slots = 416 B per cell state): what one launch must read
-# and write at least, stage mean for the residual kernel.
-ALG_BYTES_PER_CELL = {
-    "face_x": 416 + 40 * 8 + 5 * 8,          # cell modes once, Fxhat + EzRL of the cell's face
-    "face_y": 416 + 40 * 8 + 5 * 8,
-    "vertex": 416 + 8,                       # cell modes once, one vertex Ez
-    "cell": (1888 + 2 * 2304) / 3,           # U + faces' Fhat + U0/UI read, UI (+U0) written; stage mean
-    "bface": 2 * (5 * 8 + 8 + 3 * 8 * 3),    # two faces: Ez points, vertex, B/B0/BI read+written
-    "limit": 416 + 416 + 4,                  # pre-limit modes, limited modes, flag (face-B minmod on:
-                                             # the div-free reconstruction is its own kernel)
-    "limit_tvb": 416 + 416 + 4,              # per deferred (gated) cell: modes, limited modes, flag
-    "faceb_limit": 8 * 8 + 2 * 4 * 8,        # 4 Bx + 4 By modes of the cell, 2 coefficients of its 2 faces r+w
-    "divfree": 2 * 3 * 8 + 16 * 8,           # 3 coefficients of 2 owned faces, 16 B modes written
-    "set_bc": 0.0,
-    "dt": 8 * 8,                             # cell averages
-}
-# the limiter with the div-free reconstruction fused (face-B minmod off)
-ALG_BYTES_LIMIT_FUSED = 416 + 2 * 6 * 8 + 416 + 4   # + 4 face polys (2 owned)
+# Algorithmic HBM bytes per cell-update of a full step (the live state:
+# 6 P2 modes of 6 cell variables + 3 modes of the 2 owned face-B fields =
+# 42 FP64 = 336 B; 3 stages x (read + write) + 2 reads of u^n + 64 B of
+# cell averages for dt): 8 x 336 + 64. One stage's share is a third.
+STEP_BYTES_PER_CELL = 8 * 336 + 64
+STAGE_BYTES_PER_CELL = STEP_BYTES_PER_CELL / 3.0
 
 
 def read_peaks():
@@ -191,75 +199,171 @@ def reduce_max_ms(ms: float, dist, device) -> float:
     return float(t.item())
 
 
-def job_value(world: int, steps: int, ms_max: float) -> float:
+def job_value(world: int, cells: int, steps: int, ms_max: float) -> float:
     """Whole-job cell-updates/s: every rank advances its own replica."""
-    return world * NX * NY * steps / (ms_max / 1e3)
+    return world * cells * steps / (ms_max / 1e3)
 
 
-def make_state(gdf):
-    cfg, _ = gdf.problem_config(gdf.PROB_ROTOR, NX, NY)
-    uh, bx, by = gdf.init_data(cfg, gdf.PROB_ROTOR)
-    return cfg, uh, bx, by
+BAND_Y0 = 1152                 # first row of the CPU sample band
 
 
-def cpu_baseline(gdf, steps: int):
-    """The oracle (CPU restatement of the reference) on the same workload."""
+def band_config(cfg):
+    """The CPU sample of the blast: BAND rows of the same grid from row
+    BAND_Y0 (same cell size and initial data), with outflow edges of its
+    own; 3.3% of its cells lie inside the initial blast disc (r < 0.1), as
+    3.1% of the whole grid's do."""
+    b = cfg.copy()
+    h = (cfg.yb - cfg.ya) / cfg.ny
+    b.ny = BAND
+    b.ya = cfg.ya + BAND_Y0 * h
+    b.yb = cfg.ya + (BAND_Y0 + BAND) * h
+    return b
+
+
+def kernel_counters():
+    """Per-kernel ncu figures of the blast (DRAM bytes and executed FP64
+    flops per cell per launch), from the committed profile summary."""
+    p = os.path.join(REPO, "profiles", "kernel_counters_blast.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def cpu_sample(steps: int, warmup: int):
+    """The oracle (CPU restatement of the reference, OpenMP on all host
+    threads) on the band sample of the workload: `warmup` untimed steps,
+    then `steps` timed ones. No GPU library is loaded."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
+    from gdf._abi import PROB_BLAST, problem_config     # pure Python (ctypes structs), no library load
     from oracle import Oracle, set_threads
     cores = set_threads(0)
-    cfg, uh, bx, by = make_state(gdf)
-    o = Oracle(cfg)
+    cfg, tend = problem_config(PROB_BLAST, NX, NY)
+    bcfg = band_config(cfg)
+    o = Oracle(bcfg)
+    uh, bx, by = o.init_data(PROB_BLAST)
     o.prepare(uh, bx, by)
-    t, _, _ = o.step(uh, bx, by, 0.0, 1e9)          # warm-up step
+    t = 0.0
+    for _ in range(warmup):
+        t, _, _ = o.step(uh, bx, by, t, tend)
     t0 = time.perf_counter()
     for _ in range(steps):
-        t, _, _ = o.step(uh, bx, by, t, 1e9)
+        t, _, _ = o.step(uh, bx, by, t, tend)
     el = time.perf_counter() - t0
-    return {"value": NX * NY * steps / el, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"rotor {NX}x{NY} (the benchmark workload), {steps} timed steps after prepare and 1 "
-                      f"warm-up step, oracle/gdf_oracle.cpp with OpenMP on {cores} host threads",
-            "seconds": el}
+    cells = bcfg.nx * bcfg.ny
+    return {"value": cells * steps / el, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": (f"a {bcfg.nx}x{bcfg.ny} band of the 2048^2 blast, rows {BAND_Y0}-{BAND_Y0 + BAND - 1} "
+                       f"(y in [{bcfg.ya:g}, {bcfg.yb:g}]; same cell size and initial data, outflow at the band's "
+                       f"edges; 3.3% of its cells start inside the blast disc, 3.1% of the whole grid's), "
+                       f"{steps} timed full SSP-RK3 steps after prepare and "
+                       f"{warmup} untimed step(s); plain method (sticky KXRCF, the reference's); "
+                       f"oracle/gdf_oracle.cpp (-O2, no FMA, as a gfortran build of the reference) with OpenMP "
+                       f"on {cores} host threads; the reference Fortran cannot be built here (no Fortran "
+                       f"compiler)"),
+            "seconds": el, "steps": steps, "warmup": warmup}
 
 
-def learned_blast(gdf, steps: int):
-    """Plain (KXRCF) vs learned-indicator throughput on the MHD blast.
+def make_blast(gdf, detector, net=None, lo=0.5, hi=0.5, state=None):
+    cfg, tend = gdf.problem_config(gdf.PROB_BLAST, NX, NY)
+    cfg.detector = detector
+    if state is None:
+        state = gdf.init_data(cfg, gdf.PROB_BLAST)
+    s = gdf.Solver(cfg)
+    if net is not None:
+        s.set_indicator(net, lo, hi)
+    s.upload(*state)
+    s.prepare()
+    return s, cfg, tend, state
 
-    Whole runs at 512^2 (t = 0.01, every step timed) give the throughput of
-    both methods over the blast's evolution and the L1 density difference
-    learned vs plain; at 2048^2, `steps` steps from the start of the run
-    (after 3 warm-up steps) are timed for both."""
+
+def residual_roofline(prof, ncell, hbm_peak, peak_kind, fp64_tflops, counters, step_ms):
+    """Roofline of the residual kernel (the stage's main kernel, one launch
+    per stage): algorithmic bytes = one stage's share of the step's 2752 B
+    per cell; measured time = its event-timed launches."""
+    kind = "cell"
+    ms, per_step = prof[kind]
+    alg = STAGE_BYTES_PER_CELL * ncell
+    achieved = alg / (ms / 1e3) / 1e9
+    c = counters.get(kind, {})
+    traffic = c.get("dram_bytes_per_cell")
+    flops = c.get("fp64_flops_per_cell")
+    total_ms = sum(v[0] * v[1] for v in prof.values())
+    out = {"bound": "hbm", "kernel": kind, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+           "frac": achieved / hbm_peak, "traffic": (traffic * ncell) if traffic else None,
+           "peak_kind": peak_kind, "alg_bytes_per_launch": alg, "ms_per_launch": ms,
+           "launches_per_step": per_step, "share_of_step": ms * per_step / total_ms if total_ms else None,
+           "step": {"alg_bytes_per_cell_update": STEP_BYTES_PER_CELL, "ms": step_ms,
+                    "achieved_gbs": STEP_BYTES_PER_CELL * ncell / (step_ms / 1e3) / 1e9,
+                    "frac": STEP_BYTES_PER_CELL * ncell / (step_ms / 1e3) / 1e9 / hbm_peak}}
+    if traffic:
+        out["traffic_source"] = c.get("source")
+    if fp64_tflops:
+        fp = {"peak_tflops": fp64_tflops, "peak_kind": "measured (gdf_fp64_fma_peak, same run)"}
+        if flops:
+            fp["flops_per_launch"] = flops * ncell
+            fp["achieved_tflops"] = flops * ncell / (ms / 1e3) / 1e12
+            fp["frac"] = fp["achieved_tflops"] / fp64_tflops
+            fp["flops_source"] = c.get("source")
+        out["fp64"] = fp
+    return out
+
+
+def run_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    cpu = cpu_sample(args.steps, args.warmup)
+    value = cpu["value"]
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": cpu["seconds"] / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": CONFIG, "impl": "reference",
+        "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def rotor_extra(gdf, steps: int, hbm_peak, peak_kind, fp64_tflops):
+    """The plain method at scale on the MHD rotor 512^2 (HLLD, KXRCF + TVB
+    + face-B minmod + pp), and the opt-in FMA build on it."""
+    cfg, _ = gdf.problem_config(gdf.PROB_ROTOR, 512, 512)
+    state = gdf.init_data(cfg, gdf.PROB_ROTOR)
+    out = {}
+    for name, exact in (("exact", True), ("fma_build", False)):
+        s = gdf.Solver(cfg, exact=exact)
+        s.upload(*state)
+        s.prepare()
+        s.advance_timed(1e9, 3)
+        _, k, ms = s.advance_timed(1e9, steps)
+        r = {"value": 512 * 512 * k / (ms / 1e3), "ms_per_step": ms / k, "steps": k}
+        if exact:
+            prof = s.profile(2)
+            r["roofline"] = residual_roofline(prof, 512 * 512, hbm_peak, peak_kind, fp64_tflops, {}, ms / k)
+            r["kernels_ms_per_launch"] = {kk: v[0] for kk, v in prof.items() if v[1]}
+        s.close()
+        out[name] = r
+    return out
+
+
+def learned_blast512(gdf):
+    """Whole runs of the benchmark blast at 512^2 (t = 0.01, every step
+    timed) with both methods, and the L1 density difference between them."""
     from gdf.indicator import WEIGHTS, load_net, run
     import numpy as np
     net, lo, hi = load_net(WEIGHTS)
-    out = {"weights": os.path.relpath(WEIGHTS, REPO), "t_lo": lo, "t_hi": hi}
     u_p, st_p, ms_p, g_p = run(512, 0, None, params="default")
     u_l, st_l, ms_l, g_l = run(512, 0, net, lo, hi, params="default")
     rho_p, rho_l = u_p[0, 0, 1:-1, 1:-1], u_l[0, 0, 1:-1, 1:-1]
-    out["blast512_full_run"] = {
-        "plain": {"value": 512 * 512 / (ms_p / 1e3), "ms_per_step": ms_p, "steps": st_p,
-                  "gated_cells_per_step": g_p},
-        "learned": {"value": 512 * 512 / (ms_l / 1e3), "ms_per_step": ms_l, "steps": st_l,
-                    "gated_cells_per_step": g_l},
-        "speedup": ms_p * st_p / (ms_l * st_l),
-        "l1_rho_learned_vs_plain": float(np.abs(rho_l - rho_p).mean() / np.abs(rho_p).mean())}
-    n = 2048
-    res = {}
-    for name, det in (("plain", gdf.DETECT_KXRCF), ("learned", gdf.DETECT_LEARNED)):
-        cfg, tend = gdf.problem_config(gdf.PROB_BLAST, n, n)
-        cfg.detector = det
-        uh, bx, by = gdf.init_data(cfg, gdf.PROB_BLAST)
-        s = gdf.Solver(cfg)
-        if det == gdf.DETECT_LEARNED:
-            s.set_indicator(net, lo, hi)
-        s.upload(uh, bx, by)
-        s.prepare()
-        s.advance_timed(tend, 3)
-        _, k, ms = s.advance_timed(tend, steps)
-        res[name] = {"value": n * n * k / (ms / 1e3), "ms_per_step": ms / k, "steps": k}
-        s.close()
-    res["speedup"] = res["plain"]["ms_per_step"] / res["learned"]["ms_per_step"]
-    out["blast2048_first_steps"] = res
-    return out
+    return {"plain": {"value": 512 * 512 / (ms_p / 1e3), "ms_per_step": ms_p, "steps": st_p,
+                      "gated_cells_per_step": g_p},
+            "learned": {"value": 512 * 512 / (ms_l / 1e3), "ms_per_step": ms_l, "steps": st_l,
+                        "gated_cells_per_step": g_l},
+            "speedup": ms_p * st_p / (ms_l * st_l),
+            "l1_rho_learned_vs_plain": float(np.abs(rho_l - rho_p).mean() / np.abs(rho_p).mean())}
 
 
 def ensemble_bench(gdf, steps: int):
@@ -273,7 +377,6 @@ def ensemble_bench(gdf, steps: int):
     cells = [c.nx * c.ny for c, _, _, _ in items]
     states = [gdf.init_data(c, p, prm) for c, p, prm, _ in items]
     out = {"instances": len(items), "cells": int(sum(cells)), "sides": sorted({c.nx for c, _, _, _ in items})}
-    # plain, one instance at a time
     cu, tot_ms = 0, 0.0
     for (c, p, prm, tend), st in zip(items, states):
         cp = c.copy()
@@ -314,65 +417,38 @@ def ensemble_bench(gdf, steps: int):
     return out
 
 
-def run_reference(args):
-    world, rank, _ = dist_env()
-    if rank != 0:
-        return 0
-    import gdf
-    k = max(1, min(args.steps, 10))
-    w = max(0, min(args.warmup, 1))
-    sys.path.insert(0, os.path.join(REPO, "oracle"))
-    from oracle import Oracle, set_threads
-    cores = set_threads(0)
-    cfg, uh, bx, by = make_state(gdf)
-    o = Oracle(cfg)
-    o.prepare(uh, bx, by)
-    t = 0.0
-    for _ in range(w):
-        t, _, _ = o.step(uh, bx, by, t, 1e9)
-    t0 = time.perf_counter()
-    for _ in range(k):
-        t, _, _ = o.step(uh, bx, by, t, 1e9)
-    el = time.perf_counter() - t0
-    value = NX * NY * k / el
-    line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": el / k * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "grid": [NX, NY], "problem": "rotor"},
-        "impl": "reference",
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{k} steps (of --steps {args.steps}) of the rotor {NX}x{NY} after prepare "
-                                   f"and {w} warm-up step(s); the reference Fortran cannot be built here "
-                                   "(no Fortran compiler), so its CPU restatement oracle/gdf_oracle.cpp runs"},
-        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
-    print(json.dumps(line), flush=True)
-    return 0
-
-
 def run_quick(args):
     """Warm-up and timed steps only: the commands the ncu captures run.
 
-    --workload rotor           the benchmark workload (rotor 512^2, plain)
-    --workload blast-learned   blast 512^2 with the shipped learned gate
+    --workload blast           the benchmark blast, learned gate, at --n
+                               cells per side (default 512)
+    --workload blast-plain     the same with the plain method (KXRCF)
+    --workload rotor           rotor at --n, plain method
     --workload ensemble-small  8 instances (64^2..160^2, OT / rotor / blast,
                                HLLD, learned gate) in the persistent kernels
     --workload mlp-train       one epoch of indicator training on 65536
                                synthetic samples (batch 2048)"""
     import gdf
     gdf.set_device(dist_env()[2])
-    w = args.workload
-    if w == "rotor":
-        cfg, uh, bx, by = make_state(gdf)
+    w, n = args.workload, args.n
+    if w in ("blast", "blast-plain", "rotor"):
+        prob = gdf.PROB_ROTOR if w == "rotor" else gdf.PROB_BLAST
+        cfg, tend = gdf.problem_config(prob, n, n)
+        net = None
+        if w == "blast":
+            from gdf.indicator import WEIGHTS, load_net
+            net, lo, hi = load_net(WEIGHTS)
+            cfg.detector = gdf.DETECT_LEARNED
         s = gdf.Solver(cfg, exact=not args.fma)
-        s.upload(uh, bx, by)
+        if net is not None:
+            s.set_indicator(net, lo, hi)
+        s.upload(*gdf.init_data(cfg, prob))
         s.prepare()
         if args.warmup:
-            s.advance_timed(1e9, args.warmup)
-        _, n, ms = s.advance_timed(1e9, args.steps)
-        print(json.dumps({"quick": True, "workload": w, "steps": n, "ms_per_step": ms / n,
-                          "value": NX * NY * n / (ms / 1e3)}))
+            s.advance_timed(tend if w != "rotor" else 1e9, args.warmup)
+        _, k, ms = s.advance_timed(tend if w != "rotor" else 1e9, args.steps)
+        print(json.dumps({"quick": True, "workload": w, "n": n, "steps": k, "ms_per_step": ms / max(k, 1),
+                          "value": n * n * k / (ms / 1e3)}))
         s.close()
         return 0
     if w == "mlp-train":
@@ -388,25 +464,10 @@ def run_quick(args):
         return 0
     from gdf.indicator import WEIGHTS, load_net
     net, lo, hi = load_net(WEIGHTS)
-    if w == "blast-learned":
-        cfg, tend = gdf.problem_config(gdf.PROB_BLAST, 512, 512)
-        cfg.detector = gdf.DETECT_LEARNED
-        s = gdf.Solver(cfg)
-        s.set_indicator(net, lo, hi)
-        s.upload(*gdf.init_data(cfg, gdf.PROB_BLAST))
-        s.prepare()
-        if args.warmup:
-            s.advance_timed(tend, args.warmup)
-        _, n, ms = s.advance_timed(tend, args.steps)
-        print(json.dumps({"quick": True, "workload": w, "steps": n, "ms_per_step": ms / n,
-                          "value": 512 * 512 * n / (ms / 1e3)}))
-        s.close()
-        return 0
-    # ensemble-small
     items = []
-    for i, (prob, side) in enumerate([(gdf.PROB_ORSZAG_TANG, 64), (gdf.PROB_ROTOR, 96), (gdf.PROB_BLAST, 128),
-                                      (gdf.PROB_ROTOR, 160), (gdf.PROB_BLAST, 64), (gdf.PROB_ORSZAG_TANG, 128),
-                                      (gdf.PROB_ROTOR, 64), (gdf.PROB_BLAST, 96)]):
+    for prob, side in [(gdf.PROB_ORSZAG_TANG, 64), (gdf.PROB_ROTOR, 96), (gdf.PROB_BLAST, 128),
+                       (gdf.PROB_ROTOR, 160), (gdf.PROB_BLAST, 64), (gdf.PROB_ORSZAG_TANG, 128),
+                       (gdf.PROB_ROTOR, 64), (gdf.PROB_BLAST, 96)]:
         c, te = gdf.problem_config(prob, side, side)
         c.flux_type = gdf.FLUX_HLLD
         c.faceb_limiter = 1
@@ -433,6 +494,7 @@ def run_ours(args):
     world, rank, local = dist_env()
     import numpy as np
     import gdf
+    from gdf.indicator import WEIGHTS, load_net
     dist = None
     if world > 1:
         import datetime
@@ -441,11 +503,12 @@ def run_ours(args):
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     gdf.set_device(local)
-    cfg, uh, bx, by = make_state(gdf)
-    s = gdf.Solver(cfg)
-    s.upload(uh, bx, by)
-    s.prepare()
-    s.advance_timed(1e9, max(3, args.warmup))       # warm-up (also captures the step graph)
+    ncell = NX * NY
+    net, lo, hi = load_net(WEIGHTS)
+
+    # the learned-indicator method: the headline value
+    s, cfg, tend, state = make_blast(gdf, gdf.DETECT_LEARNED, net, lo, hi)
+    s.advance_timed(tend, args.warmup)              # warm-up (also captures the step graph)
     if dist:
         dist.barrier()
     clk = ClockSampler(local)
@@ -453,137 +516,131 @@ def run_ours(args):
     time.sleep(0.05)
     l0 = s.kernel_launches()
     h0 = time.perf_counter()
-    _, taken, ms = s.advance_timed(1e9, args.steps)   # returns after the device finished
+    _, taken, ms = s.advance_timed(tend, args.steps)   # returns after the device finished
     clk.mark(h0, time.perf_counter())
     launches = s.kernel_launches() - l0
-    clocks = clk.stop()
+    if taken != args.steps:
+        raise RuntimeError(f"the blast took {taken} of {args.steps} steps (end time reached or stopped)")
     ms_max = reduce_max_ms(ms, dist, f"cuda:{local}")
-    value = job_value(world, args.steps, ms_max)
+    value = job_value(world, ncell, args.steps, ms_max)
 
-    # per-kernel timing (events around every launch) for the roofline
+    # the plain method over the same steps from the same state
+    p, _, _, _ = make_blast(gdf, gdf.DETECT_KXRCF, state=state)
+    p.advance_timed(tend, args.warmup)
+    if dist:
+        dist.barrier()
+    _, taken_p, ms_p = p.advance_timed(tend, args.steps)
+    clocks = clk.stop()
+    ms_p_max = reduce_max_ms(ms_p, dist, f"cuda:{local}")
+    plain_value = job_value(world, ncell, taken_p, ms_p_max)
+    rho_l = s.download()[0][0, 0, 1:-1, 1:-1]
+    rho_p = p.download()[0][0, 0, 1:-1, 1:-1]
+    l1 = float(np.abs(rho_l - rho_p).sum() / np.abs(rho_p).sum())
+    gated = {"learned": s.diagnostics()[3], "plain": p.diagnostics()[3]}
+    p.close()
+
+    # measured FP64 ceiling (FMA-only kernel on every SM), clocks sampled
+    clk2 = ClockSampler(local)
+    clk2.start()
+    time.sleep(0.05)
+    f0 = time.perf_counter()
+    fp64_tflops, fp64_ms = gdf.fp64_fma_peak(4, 20000)
+    clk2.mark(f0, time.perf_counter())
+    fp64_clocks = clk2.stop()
+
+    # per-kernel event timing for the roofline (2 more steps, events around
+    # every launch)
     prof = s.profile(2)
-    dom = max((k for k in prof if k in ALG_BYTES_PER_CELL), key=lambda k: prof[k][0] * prof[k][1])
-    dom_ms, dom_per_step = prof[dom]
-    # with a detector the limiter runs in two passes: the first reads every
-    # cell and writes the ungated ones, the second takes the gated cells (the
-    # sticky KXRCF flags)
-    flagged = int((s.trouble() != 0).sum())
-    ncell = NX * NY
-    if dom == "limit_tvb":
-        alg_bytes = ALG_BYTES_PER_CELL["limit_tvb"] * flagged
-    elif dom == "limit":
-        alg_bytes = 416 * ncell + (416 + 4) * (ncell - flagged) + 4 * flagged
-        if not cfg.faceb_limiter:
-            alg_bytes += (ALG_BYTES_LIMIT_FUSED - ALG_BYTES_PER_CELL["limit"]) * (ncell - flagged)
-    else:
-        alg_bytes = ALG_BYTES_PER_CELL[dom] * ncell
-    peak, peak_kind = read_peaks()
-    achieved = alg_bytes / (dom_ms / 1e3) / 1e9
-    traffic = None
-    tp = os.path.join(REPO, "profiles", "traffic_rotor512.json")
-    if os.path.exists(tp):
-        try:
-            traffic = json.load(open(tp)).get(dom)
-        except Exception:
-            traffic = None
+    hbm_peak, peak_kind = read_peaks()
+    roof = residual_roofline(prof, ncell, hbm_peak, peak_kind, fp64_tflops, kernel_counters(), ms_max / args.steps)
 
-    # end to end through the public API with host buffers (pinned)
+    # end to end through the public C ABI with host buffers (pinned): every
+    # step uploads the state, steps, downloads the live state
     import torch
+    uh, bx, by = s.download()
     pin = lambda a: torch.from_numpy(a).pin_memory().numpy()   # noqa: E731
     huh, hbx, hby = pin(uh), pin(bx), pin(by)
-    s.upload(huh, hbx, hby)
-    s.prepare()
-    huh2, hbx2, hby2 = s.download()
-    huh, hbx, hby = pin(huh2), pin(hbx2), pin(hby2)
-    e2e_steps = max(2, min(args.steps, 10))
-    t = 0.0
+    del uh, bx, by
+    e2e_steps = max(2, min(args.steps, 5))
+    t = s.t
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         s.upload(huh, hbx, hby)
         s.t = t
-        t, _, _ = s.step(1e9, flags=False)
+        t, _, _ = s.step(tend, flags=False)
         s.download_into(huh, hbx, hby, live_only=True)
     e2e_el = time.perf_counter() - t0
-    e2e = world * NX * NY * e2e_steps / e2e_el
-    io_bytes = huh.nbytes + hbx.nbytes + hby.nbytes
+    e2e = world * ncell * e2e_steps / e2e_el
     # gdf_upload moves the 52 live slot planes of uh (the 28 dead ones are
     # checked to be zero on the host and stay zero on the device)
-    h2d_bytes = huh.nbytes * 52 // 80 + hbx.nbytes + hby.nbytes
-
-    # the opt-in FMA build on the same workload, for comparison
-    fma = None
-    if not args.no_fma:
-        f = gdf.Solver(cfg, exact=False)
-        f.upload(uh, bx, by)
-        f.prepare()
-        f.advance_timed(1e9, 3)
-        _, _, fms = f.advance_timed(1e9, args.steps)
-        fma = {"value": NX * NY * args.steps / (fms / 1e3), "unit": UNIT, "ms_per_step": fms / args.steps,
-               "build": "libgdf_b200_fma.so (FMA contraction; not tie-exact)"}
-        f.close()
+    io_bytes = huh.nbytes * 52 // 80 + hbx.nbytes + hby.nbytes
+    s.close()
+    del huh, hbx, hby
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(gdf, args.cpu_steps)
+        cpu = cpu_sample(args.cpu_steps, 1)
 
-    learned = ens = None
+    extras = {}
     if not args.no_extra and rank == 0 and world == 1:
-        try:
-            learned = learned_blast(gdf, args.steps)
-        except Exception as e:   # reported, not fatal: the headline line still prints
-            learned = {"error": str(e)}
-        try:
-            ens = ensemble_bench(gdf, args.steps)
-        except Exception as e:
-            ens = {"error": str(e)}
+        for name, fn in (("rotor512_plain", lambda: rotor_extra(gdf, 100, hbm_peak, peak_kind, fp64_tflops)),
+                         ("blast512_full_run", lambda: learned_blast512(gdf)),
+                         ("ensemble", lambda: ensemble_bench(gdf, args.steps))):
+            try:
+                extras[name] = fn()
+            except Exception as e:   # reported, not fatal: the headline line still prints
+                extras[name] = {"error": str(e)}
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "grid": [NX, NY], "problem": "rotor", "method": "plain",
-                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                       "l2": "inputs larger than L2 (uh alone is 168 MB per copy; 126 MB L2)",
-                       "timing": "CUDA events on the library stream around graph replays"},
+            "config": dict(CONFIG, parallelism=f"replicas x{world}" if world > 1 else "single GPU",
+                           timing="CUDA events on the library stream around graph replays"),
+            "method": "learned indicator (90-64-64-1 MLP gate, KXRCF in [t_lo, t_hi), TVB where gated)",
+            "indicator": {"weights": os.path.relpath(WEIGHTS, REPO), "t_lo": lo, "t_hi": hi},
+            "plain": {"value": plain_value, "unit": UNIT, "ms_per_step": ms_p_max / max(taken_p, 1),
+                      "steps": taken_p, "method": "sticky KXRCF detector + characteristic TVB (the reference's)"},
+            "speedup_learned_vs_plain": value / plain_value,
+            "l1_rho_learned_vs_plain": l1,
+            "gated_cells_last_step": gated,
             "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "alg_bytes_per_launch": alg_bytes, "ms_per_launch": dom_ms,
-                         "launches_per_step": dom_per_step, "flagged_cells": flagged},
+            "roofline": roof,
+            "fp64_peak": {"tflops": fp64_tflops, "ms": fp64_ms, "clocks": fp64_clocks,
+                          "kernel": "gdf_fp64_fma_peak: 4 x 256-thread blocks per SM, 8 FMA chains per thread"},
             "kernels_ms_per_launch": {k: v[0] for k, v in prof.items() if v[1]},
-            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d_bytes),
-                    "d2h_bytes_per_step": int(h2d_bytes), "steps": e2e_steps,
-                    "calls": "gdf_upload, gdf_step, gdf_download_live per step (pinned host arrays)"},
-            "cpu_baseline": cpu,
-            "fma_build": fma,
-            "learned_indicator": learned,
-            "ensemble": ens,
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(io_bytes),
+                    "d2h_bytes_per_step": int(io_bytes), "steps": e2e_steps,
+                    "calls": "gdf_upload, gdf_step, gdf_download_live per step (pinned host arrays), "
+                             "learned-indicator method"},
+            "cpu_baseline": ({k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")} if cpu else None),
             "build": "libgdf_b200.so (no FMA contraction: value-exact with the reference arithmetic)",
             "clocks": clocks,
             "steps_taken": taken,
+            "extras": extras,
         }
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
-    s.close()
     return 0
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=3)
-    ap.add_argument("--no-fma", action="store_true")
-    ap.add_argument("--no-extra", action="store_true", help="skip the learned-indicator and ensemble runs")
+    ap.add_argument("--no-extra", action="store_true", help="skip the rotor, 512^2 blast and ensemble runs")
     ap.add_argument("--quick", action="store_true", help="timed steps only (for profiler captures)")
     ap.add_argument("--fma", action="store_true", help="with --quick: run the FMA build")
-    ap.add_argument("--workload", default="rotor", choices=["rotor", "blast-learned", "ensemble-small", "mlp-train"],
+    ap.add_argument("--n", type=int, default=512, help="with --quick: cells per side")
+    ap.add_argument("--workload", default="blast",
+                    choices=["blast", "blast-plain", "rotor", "ensemble-small", "mlp-train"],
                     help="with --quick: what to run")
     args = ap.parse_args()
     if args.quick:

@@ -706,9 +706,6 @@ constexpr long long NOALLOC_MAX_FACES = 16640;  // (nx+1)*ny and nx*(ny+1); 128 
 constexpr long long NOALLOC_DOUBLES = 2 * NOALLOC_MAX_FACES * (NG * NE + NG);
 static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_DOUBLES];
 
-constexpr int NOALLOC_MAX_DEVICES = 256;
-static std::mutex g_noalloc_mu;
-static void* g_noalloc_addr[NOALLOC_MAX_DEVICES] = {nullptr};
 
 // Capture one time step (RK3.f90:60-151) of the resident state as a CUDA
 // graph; replays need no host work between steps.
@@ -969,32 +966,30 @@ int gdf_lh_noalloc(const GdfConfig* cfg, const double* d_uh, double* d_du, void*
     return fail(GDF_ERR_ARG, "gdf_lh_noalloc: grid " + std::to_string(cfg->nx) + "x" + std::to_string(cfg->ny) +
                                  " exceeds its fixed scratch: (nx+1)*ny and nx*(ny+1) must be at most " +
                                  std::to_string(NOALLOC_MAX_FACES) + " (128x128 fits); use gdf_lh");
-  int dev = 0;
-  CK(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(GDF_ERR_ARG, "device ordinal out of range");
+  // The scratch's device address and the basis tables are set up on every
+  // call rather than cached: a cudaDeviceReset between calls reloads the
+  // module, which moves the array and clears the __constant__ tables.
+  // cudaGetSymbolAddress is a host-side query; the tables (~10 KB, the same
+  // bytes for every grid) are copied stream-ordered ahead of the kernels.
   void* base = nullptr;
   {
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
-      // first call on this device: resolve the device address of the
-      // scratch array with this device current
-      void* p = nullptr;
-      cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-      if (e != cudaSuccess)
-        return fail(GDF_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
-      g_noalloc_addr[dev] = p;
-    }
-    base = g_noalloc_addr[dev];
+    cudaError_t e = cudaGetSymbolAddress(&base, g_noalloc_scratch);
+    if (e != cudaSuccess)
+      return fail(GDF_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
   }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
   Consts K;
   build_consts(*cfg, K);
-  cudaError_t eb = upload_basis_once(K);   // first call on a device only
-  if (eb != cudaSuccess) return fail(GDF_ERR_CUDA, std::string("basis tables: ") + cudaGetErrorString(eb));
+  {
+    Basis B;
+    basis_of(K, B);
+    cudaError_t e = cudaMemcpyToSymbolAsync(c_basis, &B, sizeof(Basis), 0, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return fail(GDF_ERR_CUDA, std::string("basis tables: ") + cudaGetErrorString(e));
+  }
   double* Fxh = static_cast<double*>(base);
   double* Fyh = Fxh + fx * NG * NE;
   double* ezx = Fyh + fy * NG * NE;
   double* ezy = ezx + fx * NG;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
   // every face point of Fxh/Fyh/Ez is written before k_cell reads it, so
   // the scratch left by an earlier call needs no clearing; du's ghost and
   // dead slots must read 0

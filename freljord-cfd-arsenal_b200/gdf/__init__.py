@@ -90,6 +90,7 @@ def load(exact: bool = True):
     L.gdf_advance_timed.argtypes = [vp, C.c_double, i32, dp, ip, dp]
     L.gdf_set_device.argtypes = [i32]
     L.gdf_lh_noalloc.argtypes = [cfgp, vp, vp, vp]
+    L.gdf_fp64_fma_peak.argtypes = [i32, i32, dp, dp]
     cp = C.c_char_p
     L.gdf_save_solution.argtypes = [cfgp, dp, cp]
     L.gdf_save_frame.argtypes = [cfgp, dp, C.c_double, cp, i32]
@@ -148,6 +149,15 @@ def lh_noalloc(cfg: GdfConfig, d_uh: int, d_du: int, stream: int = 0, exact: boo
     integers), enqueued on `stream`; allocates no device memory."""
     L = load(exact)
     _check(L, L.gdf_lh_noalloc(C.byref(cfg), C.c_void_p(d_uh), C.c_void_p(d_du), C.c_void_p(stream or None)))
+
+
+def fp64_fma_peak(blocks_per_sm: int = 4, iters: int = 20000, exact: bool = True):
+    """gdf_fp64_fma_peak: (TFLOP/s, ms) of an FMA-only kernel on every SM of
+    the current device, timed with CUDA events."""
+    L = load(exact)
+    tf, ms = C.c_double(), C.c_double()
+    _check(L, L.gdf_fp64_fma_peak(blocks_per_sm, iters, C.byref(tf), C.byref(ms)))
+    return tf.value, ms.value
 
 
 def c_problem_config(problem: int, nx: int, ny: int, exact: bool = True):

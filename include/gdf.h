@@ -284,12 +284,16 @@ const char *gdf_ens_last_error(void);
  * (the face fluxes) is a fixed array compiled into this library, so every
  * GPU that loads the library holds ~12 MB until the process exits, and the
  * grid is limited to (nx+1)*ny <= 16640 and nx*(ny+1) <= 16640 faces
- * (128 x 128 fits); larger grids get GDF_ERR_ARG. The first call on a
- * device resolves the scratch's device address with that device current;
- * make that first call before any stream capture. Work is enqueued on
- * `stream` (a cudaStream_t, NULL for the default stream) and the call
- * returns without synchronising. All calls share the one scratch array:
- * calls that overlap on the GPU (other streams, other threads) race. */
+ * (128 x 128 fits); larger grids get GDF_ERR_ARG. Each call looks up the
+ * scratch's device address for the current device and enqueues a ~10 KB
+ * copy of the basis tables on `stream` ahead of its kernels, so calls stay
+ * correct across a cudaDeviceReset. The first call on a device can also
+ * load the library's device code there; make it before any stream capture.
+ * Work is enqueued on `stream` (a cudaStream_t, NULL for the default
+ * stream) and the call returns without synchronising. All calls share the
+ * one scratch array, which keeps what the last call left (a call writes
+ * every scratch entry it reads): calls that overlap on the GPU (other
+ * streams, other threads) race, so serialise them on one stream per GPU. */
 int gdf_lh_noalloc(const GdfConfig *cfg, const double *d_uh, double *d_du, void *stream);
 
 /* calculate_umax.f90, calculate_totaldiv.f90, calculate_pmin.f90 on the
@@ -307,6 +311,14 @@ int64_t gdf_kernel_launches(GdfHandle *h);
 /* The handle's CUDA stream (a cudaStream_t), for callers that time or
  * order work against it. No counterpart in the reference. */
 void *gdf_stream(GdfHandle *h);
+
+/* Measured FP64 ceiling for the roofline of this FP64-bound step (no
+ * counterpart in the reference): runs an FMA-only kernel (independent
+ * fused multiply-add chains, no memory traffic in its loop) with
+ * blocks_per_sm blocks of 256 threads on every SM of the current device,
+ * `iters` x 128 FMAs per thread, and returns its rate in TFLOP/s (2 flops
+ * per FMA) and its CUDA-event time. Allocates and frees a small buffer. */
+int gdf_fp64_fma_peak(int32_t blocks_per_sm, int32_t iters, double *tflops, double *ms);
 
 /* Kernel kinds reported by gdf_profile. */
 enum {

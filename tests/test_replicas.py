@@ -21,7 +21,7 @@ def _worker(rank, world, port, q):
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     ms = 10.0 + 5.0 * rank          # rank 1 is the slow one
     m = bench.reduce_max_ms(ms, dist, "cpu")
-    v = bench.job_value(world, 4, m)
+    v = bench.job_value(world, bench.NX * bench.NY, 4, m)
     dist.barrier()
     dist.destroy_process_group()
     q.put((rank, m, v))
@@ -50,6 +50,30 @@ def test_reference_arm_nonzero_rank_exits_quietly():
                         "--steps", "1", "--warmup", "0"], capture_output=True, text=True, env=env, timeout=120)
     assert r.returncode == 0
     assert r.stdout.strip() == ""
+
+
+def test_cpu_sample_band_is_a_slice_of_the_blast_grid():
+    """The reference arm's band has the blast grid's cell size, its cells
+    sit on the blast grid's cell centres, and its share of cells inside the
+    initial blast disc is close to the whole grid's."""
+    import numpy as np
+    import bench
+    from gdf._abi import PROB_BLAST, problem_config
+    cfg, _ = problem_config(PROB_BLAST, bench.NX, bench.NY)
+    b = bench.band_config(cfg)
+    h = (cfg.yb - cfg.ya) / cfg.ny
+    assert (b.nx, b.ny) == (cfg.nx, bench.BAND)
+    assert abs((b.yb - b.ya) / b.ny - h) < 1e-15 and (b.xa, b.xb) == (cfg.xa, cfg.xb)
+    yc_band = b.ya + (np.arange(b.ny) + 0.5) * h
+    yc_full = cfg.ya + (np.arange(cfg.ny) + 0.5) * h
+    assert np.allclose(yc_band, yc_full[bench.BAND_Y0:bench.BAND_Y0 + bench.BAND], atol=1e-14)
+    xc = cfg.xa + (np.arange(cfg.nx) + 0.5) * h
+
+    def share(yc):
+        X, Y = np.meshgrid(xc, yc)
+        return float(((X * X + Y * Y) < 0.01).mean())
+    s_band, s_full = share(yc_band), share(yc_full)
+    assert abs(s_band - s_full) < 0.005, (s_band, s_full)
 
 
 def test_single_rank_reduce_is_identity():

@@ -2,12 +2,12 @@
 memory (their memory is planned at start-up, or a framework pool forbids
 allocations outside it). It runs on caller-owned device buffers with the
 face-flux scratch in a fixed array inside the library. Checked through the
-C ABI against the existing entry point gdf_lh, on two calls in a row with
-different grids, so the second call reuses scratch the first one left.
+C ABI against the existing entry point gdf_lh on three calls in a row. The
+first call fills the scratch; the second and third use grids whose face
+planes sit at other offsets, so both read scratch that an earlier call left
+non-zero, and a face point a call failed to write would show up there.
 This file sorts last so that a run stopping at the first failure has run
 every other test before it."""
-import ctypes as C
-
 import numpy as np
 import pytest
 
@@ -26,10 +26,11 @@ def _state(problem, nx, ny):
     return cfg, uh
 
 
-def test_lh_noalloc_matches_gdf_lh_on_two_calls():
+def test_lh_noalloc_matches_gdf_lh_on_consecutive_calls():
     import torch
     stream = torch.cuda.current_stream()
-    for problem, nx, ny in ((gdf.PROB_ROTOR, 20, 20), (gdf.PROB_ORSZAG_TANG, 24, 16)):
+    grids = ((gdf.PROB_ROTOR, 40, 36), (gdf.PROB_ORSZAG_TANG, 24, 16), (gdf.PROB_BLAST, 18, 30))
+    for problem, nx, ny in grids:
         cfg, uh = _state(problem, nx, ny)
         ref = gdf.Solver(cfg).lh(uh)                 # existing entry point (product build)
         d_uh = torch.from_numpy(uh).to("cuda")
@@ -39,7 +40,7 @@ def test_lh_noalloc_matches_gdf_lh_on_two_calls():
         stream.synchronize()
         du = d_du.cpu().numpy()
         # the product build's tolerance: value for value
-        assert np.array_equal(du, ref)
+        assert np.array_equal(du, ref), f"grid {nx}x{ny}"
 
 
 def test_lh_noalloc_rejects_grids_beyond_its_scratch():
