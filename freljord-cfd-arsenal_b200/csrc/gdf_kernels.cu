@@ -484,6 +484,9 @@ static int check_config(const GdfConfig* c) {
 }
 
 namespace gdf {
+// gdf_init.cu: the device projection of the initial data
+int init_data_device(const GdfConfig& cfg, int problem, const double* params, double* U, double* BX, double* BY,
+                     cudaStream_t st, std::string& err);
 // the message gdf_last_error() returns, for the host-only parts of the ABI
 int set_last_error(int code, const char* msg) { return fail(code, msg); }
 void consts_for(const GdfConfig& c, Consts& K) { build_consts(c, K); }
@@ -999,6 +1002,22 @@ int gdf_lh_noalloc(const GdfConfig* cfg, const double* d_uh, double* d_du, void*
   k_cell<<<nblk(K.plane, CELL_BS), CELL_BS, 0, st>>>(K, d_uh, nullptr, nullptr, Fxh, Fyh, d_du, nullptr, 0);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(GDF_ERR_CUDA, std::string("gdf_lh_noalloc launch: ") + cudaGetErrorString(e));
+  return GDF_OK;
+}
+
+// init_data.f90 on the device, into the handle's resident state.
+int gdf_init_data_device(GdfHandle* h, int32_t problem, const double* params) {
+  if (!h) return fail(GDF_ERR_ARG, "null handle");
+  if (problem < GDF_PROB_VORTEX || problem > GDF_PROB_CLOUD_SHOCK) return fail(GDF_ERR_ARG, "unknown problem");
+  CK(cudaMemsetAsync(h->U, 0, uh_bytes(h->cfg), h->st));
+  std::string err;
+  int rc = gdf::init_data_device(h->cfg, problem, params, h->U, h->BX, h->BY, h->st, err);
+  if (rc) {
+    cudaStreamSynchronize(h->st);
+    return fail(rc, err);
+  }
+  CK(cudaStreamSynchronize(h->st));
+  h->uploaded = 1;
   return GDF_OK;
 }
 

@@ -91,6 +91,7 @@ def load(exact: bool = True):
     L.gdf_set_device.argtypes = [i32]
     L.gdf_lh_noalloc.argtypes = [cfgp, vp, vp, vp]
     L.gdf_fp64_fma_peak.argtypes = [i32, i32, dp, dp]
+    L.gdf_init_data_device.argtypes = [vp, i32, dp]
     cp = C.c_char_p
     L.gdf_save_solution.argtypes = [cfgp, dp, cp]
     L.gdf_save_frame.argtypes = [cfgp, dp, C.c_double, cp, i32]
@@ -233,6 +234,12 @@ class Solver:
 
     def upload(self, uh, bx, by) -> None:
         _check(self.L, self.L.gdf_upload(self.h, dptr(uh), dptr(bx), dptr(by)))
+
+    def init_device(self, problem: int, params=None) -> None:
+        """gdf_init_data_device: the problem's initial data projected on the
+        device into the resident state (no host state, no upload)."""
+        p = None if params is None else dptr(np.ascontiguousarray(params, np.float64))
+        _check(self.L, self.L.gdf_init_data_device(self.h, problem, p))
 
     def download(self):
         uh, bx, by = new_state(self.nx, self.ny)

@@ -171,6 +171,14 @@ int gdf_advance_timed(GdfHandle *h, double tend, int32_t steps, double *t,
  * library (one process per GPU; call before gdf_create). */
 int gdf_set_device(int32_t device);
 
+/* init_data.f90:21-121 on the device, written straight into the handle's
+ * resident state (replaces gdf_init_data + gdf_upload for a large grid or
+ * an ensemble: nothing crosses the bus but a few coefficient tables).
+ * problem and params as gdf_init_data; the values equal gdf_init_data's
+ * bit for bit for every problem but GDF_PROB_VORTEX, whose exp runs on the
+ * device (within a couple of units in the last place). Synchronous. */
+int gdf_init_data_device(GdfHandle *h, int32_t problem, const double *params);
+
 /* Fine-grained drop-ins on caller arrays (uploaded, computed, downloaded).
  * gdf_lh:   Lh.f90 (du for all cells; ghost entries 0). uh ghosts are used
  *           as given, as Lh does.
