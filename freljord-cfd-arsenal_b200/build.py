@@ -30,6 +30,7 @@ MLP_SRC = os.path.join(CSRC, "gdf_mlp.cu")
 ENS_SRC = os.path.join(CSRC, "gdf_ensemble.cu")
 PEAK_SRC = os.path.join(CSRC, "gdf_peak.cu")
 INIT_SRC = os.path.join(CSRC, "gdf_init.cu")
+MLPTC_SRC = os.path.join(CSRC, "gdf_mlp_tc.cu")
 HOST_SRC = os.path.join(CSRC, "gdf_host.cpp")
 IO_SRC = os.path.join(CSRC, "gdf_io.cpp")
 HEADERS = [os.path.join(CSRC, f) for f in ("gdf_physics.cuh", "gdf_kernels.cuh", "gdf_device.cuh",
@@ -76,7 +77,7 @@ def build(verbose: bool = False, jobs: int | None = None) -> dict:
     for name, flags in (("libgdf_b200.so", ["--fmad=false", "-DGDF_EXACT=1"]),
                         ("libgdf_b200_fma.so", ["--fmad=true"])):
         objs = []
-        for src in (KERNEL_SRC, MLP_SRC, ENS_SRC, PEAK_SRC, INIT_SRC):
+        for src in (KERNEL_SRC, MLP_SRC, ENS_SRC, PEAK_SRC, INIT_SRC, MLPTC_SRC):
             obj = os.path.join(BUILD, name.replace(".so", "") + "_" + os.path.basename(src).replace(".cu", ".o"))
             if _stale(obj, [src] + HEADERS):
                 cmd = [nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17", *flags,

@@ -27,6 +27,14 @@
 
 using namespace gdf;
 
+namespace gdf {
+// gdf_mlp_tc.cu: the training tile on tcgen05 (128 samples per CTA)
+int mlp_tc_samples_per_block();
+cudaError_t mlp_fwdbwd_tc_launch(const MlpDev* D, const __nv_bfloat16* X, const float* y, const int* idx, int nsel,
+                                 float pos_w, float inv_b, float* partial, float* loss_part, int* err,
+                                 cudaStream_t st);
+}  // namespace gdf
+
 namespace {
 
 thread_local std::string g_mlp_err;
@@ -415,7 +423,12 @@ struct GdfMlp {
   int* idx = nullptr;
   long long cap = 0;
   long long adam_t = 0;
+  int tc = 1;                 // products: 1 tcgen05 (UMMA, TMEM), 0 mma.sync
+  int* err = nullptr;         // set by a tcgen05 tile whose bounded wait gave up
 };
+
+// samples per training block of the selected products
+static int mlp_tile(const GdfMlp* m) { return m->tc ? mlp_tc_samples_per_block() : TB; }
 
 static int mlp_ensure(GdfMlp* m, long long n, int blocks) {
   if (n > m->cap) {
@@ -461,13 +474,38 @@ static int fwdbwd_attr() {
   return GDF_OK;
 }
 
+// forward + backward of nsel samples (idx) into m->partial / loss_part
+static int fwdbwd_launch(GdfMlp* m, const int* idx, long long nsel, float pos_w, float inv_b, int& nb) {
+  nb = (int)((nsel + mlp_tile(m) - 1) / mlp_tile(m));
+  if (m->tc) {
+    MCK(mlp_fwdbwd_tc_launch(m->D, m->X, m->y, idx, (int)nsel, pos_w, inv_b, m->partial, m->loss_part, m->err,
+                             m->st));
+  } else {
+    int rc = fwdbwd_attr();
+    if (rc) return rc;
+    k_mlp_fwdbwd<<<nb, MLP_THREADS, sizeof(FwdSmem), m->st>>>(m->D, m->X, m->y, idx, (int)nsel, pos_w, inv_b,
+                                                              m->partial, m->loss_part);
+    MCK(cudaGetLastError());
+  }
+  return GDF_OK;
+}
+
+// the error word of the tcgen05 tiles (read back after a synchronisation)
+static int check_err(GdfMlp* m) {
+  int e = 0;
+  MCK(cudaMemcpyAsync(&e, m->err, sizeof(int), cudaMemcpyDeviceToHost, m->st));
+  MCK(cudaStreamSynchronize(m->st));
+  if (e) {
+    MCK(cudaMemsetAsync(m->err, 0, sizeof(int), m->st));
+    return mfail(GDF_ERR_TIMEOUT, "a tensor-core training tile gave up waiting for its products");
+  }
+  return GDF_OK;
+}
+
 static int mlp_grad_launch(GdfMlp* m, long long nsel, float pos_w, float inv_b) {
-  const int nb = (int)((nsel + TB - 1) / TB);
-  int rc = fwdbwd_attr();
+  int nb = 0;
+  int rc = fwdbwd_launch(m, m->idx, nsel, pos_w, inv_b, nb);
   if (rc) return rc;
-  k_mlp_fwdbwd<<<nb, MLP_THREADS, sizeof(FwdSmem), m->st>>>(m->D, m->X, m->y, m->idx, (int)nsel, pos_w, inv_b,
-                                                            m->partial, m->loss_part);
-  MCK(cudaGetLastError());
   k_mlp_reduce<<<(MLP_NPARAM + 255) / 256, 256, 0, m->st>>>(m->partial, nb, m->grad, m->loss_part, m->loss);
   MCK(cudaGetLastError());
   return GDF_OK;
@@ -487,6 +525,7 @@ int gdf_mlp_create(int32_t seed, GdfMlp** out) {
   ok = ok && cudaMalloc((void**)&m->grad, MLP_NPARAM * sizeof(float)) == cudaSuccess;
   ok = ok && cudaMalloc((void**)&m->loss, sizeof(float)) == cudaSuccess;
   ok = ok && cudaMalloc((void**)&m->D, sizeof(MlpDev)) == cudaSuccess;
+  ok = ok && cudaMalloc((void**)&m->err, sizeof(int)) == cudaSuccess && cudaMemset(m->err, 0, sizeof(int)) == cudaSuccess;
   if (!ok) {
     cudaGetLastError();
     gdf_mlp_destroy(m);
@@ -514,7 +553,7 @@ int gdf_mlp_create(int32_t seed, GdfMlp** out) {
 
 int gdf_mlp_destroy(GdfMlp* m) {
   if (!m) return GDF_OK;
-  void* bufs[] = {m->P, m->M, m->V, m->grad, m->loss, m->D, m->partial, m->loss_part, m->X, m->y, m->idx};
+  void* bufs[] = {m->P, m->M, m->V, m->grad, m->loss, m->D, m->partial, m->loss_part, m->X, m->y, m->idx, m->err};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (m->st) cudaStreamDestroy(m->st);
@@ -544,7 +583,7 @@ int gdf_mlp_get_params(GdfMlp* m, float* params) {
 int gdf_mlp_grad(GdfMlp* m, const float* X, const float* y, int64_t n, float pos_weight, float* grad,
                  float* loss) {
   if (!m || !X || !y || !grad || n < 1) return mfail(GDF_ERR_ARG, "bad argument");
-  const int nb = (int)((n + TB - 1) / TB);
+  const int nb = (int)((n + mlp_tile(m) - 1) / mlp_tile(m));
   int rc = mlp_ensure(m, n, nb);
   if (rc) return rc;
   if ((rc = mlp_upload_x(m, X, n))) return rc;
@@ -556,13 +595,13 @@ int gdf_mlp_grad(GdfMlp* m, const float* X, const float* y, int64_t n, float pos
   MCK(cudaMemcpyAsync(grad, m->grad, MLP_NPARAM * sizeof(float), cudaMemcpyDeviceToHost, m->st));
   if (loss) MCK(cudaMemcpyAsync(loss, m->loss, sizeof(float), cudaMemcpyDeviceToHost, m->st));
   MCK(cudaStreamSynchronize(m->st));
-  return GDF_OK;
+  return check_err(m);
 }
 
 int gdf_mlp_train(GdfMlp* m, const float* X, const float* y, int64_t n, int32_t epochs, int32_t batch, float lr,
                   float pos_weight, int32_t seed, float* epoch_loss) {
   if (!m || !X || !y || n < 1 || epochs < 1 || batch < TB) return mfail(GDF_ERR_ARG, "bad argument");
-  const int nb_max = (batch + TB - 1) / TB;
+  const int nb_max = (batch + mlp_tile(m) - 1) / mlp_tile(m);
   int rc = mlp_ensure(m, n, nb_max);
   if (rc) return rc;
   if ((rc = mlp_upload_x(m, X, n))) return rc;
@@ -580,11 +619,8 @@ int gdf_mlp_train(GdfMlp* m, const float* X, const float* y, int64_t n, int32_t 
     double ep_loss = 0.0;
     for (long long off = 0; off < n; off += batch) {
       const long long nsel = std::min<long long>(batch, n - off);
-      const int nb = (int)((nsel + TB - 1) / TB);
-      k_mlp_fwdbwd<<<nb, MLP_THREADS, sizeof(FwdSmem), m->st>>>(m->D, m->X, m->y, m->idx + off, (int)nsel,
-                                                                 pos_weight, 1.f / (float)nsel, m->partial,
-                                                                 m->loss_part);
-      MCK(cudaGetLastError());
+      int nb = 0;
+      if ((rc = fwdbwd_launch(m, m->idx + off, nsel, pos_weight, 1.f / (float)nsel, nb))) return rc;
       k_mlp_reduce<<<(MLP_NPARAM + 255) / 256, 256, 0, m->st>>>(m->partial, nb, m->grad, m->loss_part, m->loss);
       m->adam_t += 1;
       const float c1 = 1.f - std::pow(b1, (float)m->adam_t), c2 = 1.f - std::pow(b2, (float)m->adam_t);
@@ -596,6 +632,7 @@ int gdf_mlp_train(GdfMlp* m, const float* X, const float* y, int64_t n, int32_t 
       ep_loss += (double)l * (double)nsel;
     }
     if (epoch_loss) epoch_loss[ep] = (float)(ep_loss / (double)n);
+    if ((rc = check_err(m))) return rc;
   }
   return GDF_OK;
 }
@@ -612,6 +649,13 @@ int gdf_mlp_predict(GdfMlp* m, const float* X, int64_t n, float* p) {
   MCK(cudaMemcpyAsync(p, dp, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, m->st));
   MCK(cudaFreeAsync(dp, m->st));
   MCK(cudaStreamSynchronize(m->st));
+  return GDF_OK;
+}
+
+// products of the training step: 1 tcgen05 (default), 0 mma.sync
+int gdf_mlp_set_products(GdfMlp* m, int32_t tcgen05) {
+  if (!m || (tcgen05 != 0 && tcgen05 != 1)) return mfail(GDF_ERR_ARG, "bad argument");
+  m->tc = tcgen05;
   return GDF_OK;
 }
 

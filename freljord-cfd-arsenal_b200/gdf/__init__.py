@@ -112,6 +112,7 @@ def load(exact: bool = True):
     L.gdf_mlp_train.argtypes = [vp, fp, fp, C.c_int64, i32, i32, C.c_float, C.c_float, i32, fp]
     L.gdf_mlp_predict.argtypes = [vp, fp, C.c_int64, fp]
     L.gdf_mlp_last_error.restype = C.c_char_p
+    L.gdf_mlp_set_products.argtypes = [vp, i32]
     L.gdf_set_indicator.argtypes = [vp, vp, C.c_float, C.c_float]
     L.gdf_ens_create.argtypes = [cfgp, i32, C.POINTER(vp)]
     L.gdf_ens_destroy.argtypes = [vp]
@@ -392,6 +393,11 @@ class Mlp:
             self.close()
         except Exception:
             pass
+
+    def set_products(self, tcgen05: bool) -> None:
+        """gdf_mlp_set_products: training products on tcgen05 (True, the
+        default) or mma.sync (False)."""
+        self._ck(self.L.gdf_mlp_set_products(self.h, 1 if tcgen05 else 0))
 
     def params(self) -> np.ndarray:
         p = np.zeros(MLP_NPARAM, np.float32)

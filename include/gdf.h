@@ -218,6 +218,14 @@ int gdf_mlp_grad(GdfMlp *m, const float *X, const float *y, int64_t n, float pos
 int gdf_mlp_train(GdfMlp *m, const float *X, const float *y, int64_t n, int32_t epochs,
                   int32_t batch, float lr, float pos_weight, int32_t seed, float *epoch_loss);
 int gdf_mlp_predict(GdfMlp *m, const float *X, int64_t n, float *p);
+/* Products of the training step (no counterpart in the reference): 1 (the
+ * default) runs the five matrix products of a 128-sample tile as tcgen05
+ * UMMAs with BF16 operands in shared memory and FP32 accumulators in tensor
+ * memory; 0 runs them as mma.sync m16n8k16 tiles (64 samples per block).
+ * Same roundings either way; only the order of the FP32 sums inside a
+ * product differs. A tcgen05 tile that waits more than 2 s for its products
+ * gives up, and the training call returns GDF_ERR_TIMEOUT. */
+int gdf_mlp_set_products(GdfMlp *m, int32_t tcgen05);
 const char *gdf_mlp_last_error(void);
 /* Use the network m (copied) as the troubled-cell detector of h when its
  * config has detector GDF_DETECT_LEARNED: the limiter runs where p >= t_hi,

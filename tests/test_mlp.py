@@ -140,12 +140,14 @@ def test_rounded_model_close_to_fp64_model():
 # ------------------------------------------------------------- GPU part ----
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("n", [1, 63, 64, 200, 4096])
-def test_gpu_gradient_matches_numpy(n):
+@pytest.mark.parametrize("tc", [True, False], ids=["tcgen05", "mma_sync"])
+@pytest.mark.parametrize("n", [1, 63, 64, 127, 128, 200, 4096])
+def test_gpu_gradient_matches_numpy(n, tc):
     import gdf
     p = glorot(6).astype(np.float32)
     X, y = batch(7 + n, n)
     m = gdf.Mlp(0)
+    m.set_products(tc)
     m.set_params(p)
     assert np.array_equal(m.params(), p)
     g, loss = m.grad(X, y, pos_weight=4.0)
@@ -172,11 +174,13 @@ def test_gpu_predict_matches_numpy():
 
 
 @pytest.mark.gpu
-def test_gpu_training_learns_a_separable_rule():
+@pytest.mark.parametrize("tc", [True, False], ids=["tcgen05", "mma_sync"])
+def test_gpu_training_learns_a_separable_rule(tc):
     import gdf
     X, y = batch(10, 16384)
     Xt, yt = batch(11, 4096)
     m = gdf.Mlp(3)
+    m.set_products(tc)
     acc0 = np.mean((m.predict(Xt) > 0.5) == (yt > 0.5))
     losses = m.train(X, y, epochs=8, batch=512, lr=2e-3, seed=1)
     assert losses[-1] < 0.5 * losses[0]
