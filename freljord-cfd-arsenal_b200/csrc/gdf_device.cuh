@@ -81,22 +81,13 @@ template <int DIR>
 __host__ __device__ __forceinline__ long long face_items(const Consts& K) {
   return DIR == 0 ? (long long)(K.nx + 1) * NG * K.ny : (long long)K.nx * NG * (K.ny + 1);
 }
-template <int DIR>
-__device__ __forceinline__ void face_item(const Consts& K, const double* __restrict__ U, double* __restrict__ Fh_out,
-                                          double* __restrict__ Ez_out, long long item) {
-  const int nf = DIR == 0 ? K.nx + 1 : K.nx;
-  const int i0 = (int)(item % nf);
-  const long long r = item / nf;
-  const int g = (int)(r % NG);
-  const int j0 = (int)(r / NG);
-  long long cL, cR;
-  if (DIR == 0) {
-    cL = i0 + (long long)K.nx2 * (j0 + 1);
-    cR = cL + 1;
-  } else {
-    cL = (i0 + 1) + (long long)K.nx2 * j0;
-    cR = cL + K.nx2;
-  }
+// One face quadrature point from the modes of its two cells, read through
+// mL(n, d) (the cell on the low side) and mR(n, d) (the high side); o is the
+// face's offset in its plane. The arithmetic is that of Lh.f90:72-265 and
+// LhEz.f90:6-31 whichever memory the modes come from.
+template <int DIR, class ML, class MR>
+__device__ __forceinline__ void face_point(const Consts& K, ML mL, MR mR, int g, double* __restrict__ Fh_out,
+                                           double* __restrict__ Ez_out, long long o) {
   double uL[NE], uR[NE];
 #pragma unroll
   for (int n = 0; n < NE; ++n) {
@@ -104,11 +95,10 @@ __device__ __forceinline__ void face_item(const Consts& K, const double* __restr
 #pragma unroll
     for (int d = 0; d < NP; ++d) {
       if (!live_mode(n, d)) continue;
-      const long long off = K.plane * (d + 10 * n);
       const double pl = DIR == 0 ? c_basis.phiGR[g][d] : c_basis.phiGU[g][d];
       const double pr = DIR == 0 ? c_basis.phiGL[g][d] : c_basis.phiGD[g][d];
-      a = a + U[off + cL] * pl;
-      b = b + U[off + cR] * pr;
+      a = a + mL(n, d) * pl;
+      b = b + mR(n, d) * pr;
     }
     uL[n] = a;
     uR[n] = b;
@@ -119,7 +109,6 @@ __device__ __forceinline__ void face_item(const Consts& K, const double* __restr
   double Fh[NE], fL[NE], fR[NE];
   face_flux_sides(K.P, L, R, DIR, Fh, fL, fR);
   const long long fp = DIR == 0 ? K.fxplane : K.fyplane;
-  const long long o = i0 + (long long)nf * j0;
 #pragma unroll
   for (int n = 0; n < NE; ++n) Fh_out[(n * NG + g) * fp + o] = Fh[n];
   double ez;
@@ -139,6 +128,63 @@ __device__ __forceinline__ void face_item(const Consts& K, const double* __restr
     }
   }
   Ez_out[g * fp + o] = ez;
+}
+
+template <int DIR>
+__device__ __forceinline__ void face_item(const Consts& K, const double* __restrict__ U, double* __restrict__ Fh_out,
+                                          double* __restrict__ Ez_out, long long item) {
+  const int nf = DIR == 0 ? K.nx + 1 : K.nx;
+  const int i0 = (int)(item % nf);
+  const long long r = item / nf;
+  const int g = (int)(r % NG);
+  const int j0 = (int)(r / NG);
+  long long cL, cR;
+  if (DIR == 0) {
+    cL = i0 + (long long)K.nx2 * (j0 + 1);
+    cR = cL + 1;
+  } else {
+    cL = (i0 + 1) + (long long)K.nx2 * j0;
+    cR = cL + K.nx2;
+  }
+  const long long pl = K.plane;
+  face_point<DIR>(
+      K, [&](int n, int d) { return U[pl * (d + 10 * n) + cL]; }, [&](int n, int d) { return U[pl * (d + 10 * n) + cR]; },
+      g, Fh_out, Ez_out, i0 + (long long)nf * j0);
+}
+
+// Faces of one block, staged: FACE_TILE faces of one face row at all NG
+// points (FACE_TILE * NG threads of a 128-thread block). The modes of the
+// cells they touch are copied once into shared memory with coalesced loads
+// (x faces: the FACE_TILE + 1 cells of one cell row; y faces: FACE_TILE
+// cells of the two cell rows), and every face point reads its two cells
+// from there instead of issuing 104 scattered global loads of its own.
+constexpr int FACE_TILE = 25;
+constexpr int FACE_TILE_W = FACE_TILE + 1;   // cells per staged row
+template <int DIR>
+__device__ __forceinline__ void face_tile(const Consts& K, const double* __restrict__ U, double* __restrict__ Fh_out,
+                                          double* __restrict__ Ez_out, int f0, int j0,
+                                          double (*ms)[2 * FACE_TILE_W]) {
+  const int nf = DIR == 0 ? K.nx + 1 : K.nx;
+  const int rows = DIR == 0 ? 1 : 2;
+  const int ncx = DIR == 0 ? min(FACE_TILE_W, nf + 1 - f0) : min(FACE_TILE, nf - f0);
+  const long long pl = K.plane;
+  const int per_slot = rows * ncx;
+  for (int q = threadIdx.x; q < NLIVE * per_slot; q += blockDim.x) {
+    const int s = q / per_slot, rk = q - s * per_slot;
+    const int r = rk / ncx, k = rk - r * ncx;
+    const long long cell = DIR == 0 ? f0 + k + (long long)K.nx2 * (j0 + 1) : (f0 + 1 + k) + (long long)K.nx2 * (j0 + r);
+    ms[s][r * FACE_TILE_W + k] = U[cell + pl * (c_live_d[s] + 10 * c_live_n[s])];
+  }
+  __syncthreads();
+  const int t = threadIdx.x;
+  if (t >= FACE_TILE * NG) return;
+  const int f = t % FACE_TILE, g = t / FACE_TILE;
+  const int i0 = f0 + f;
+  if (i0 >= nf) return;
+  const int kR = DIR == 0 ? f + 1 : FACE_TILE_W + f;
+  face_point<DIR>(
+      K, [&](int n, int d) { return ms[LI(n, d)][f]; }, [&](int n, int d) { return ms[LI(n, d)][kR]; }, g, Fh_out,
+      Ez_out, i0 + (long long)nf * j0);
 }
 
 // ------------------------------------------------------- vertex Ez -------
@@ -494,12 +540,31 @@ __device__ __forceinline__ void gather_features(const Consts& K, const float* __
 // fused, for one interior cell. S is the pre-limit state (ghosts as the
 // reference leaves them), D receives the limited state.
 constexpr int LIM_BS = 64;
+// the second limiter pass (gated cells only) with rolled 8x8 products and
+// one out-of-line eigenmatrix (same arithmetic, smaller instruction stream)
+#ifndef GDF_TVB_ROLLED
+#define GDF_TVB_ROLLED true
+#endif
 // dynamic shared memory of a learned-mode limiter block: X, W1t, W2t, H1
 // tiles (BF16) and the LIM_BS logits
 constexpr size_t LIMIT_SMEM_LEARNED = (size_t)(LIM_BS + MLP_H) * MLP_LDX * 2 + (size_t)(MLP_H + LIM_BS) * MLP_LDH * 2 +
                                       LIM_BS * sizeof(float);
 
+template <bool ROLLED = false>
 __device__ __forceinline__ void matvec8(const double* A, const double* x, double* y) {
+  if (ROLLED) {
+    // the same sums with the row loop kept as a loop: the second limiter
+    // pass (k_limit_tvb) waits on instruction fetch when its twelve 8x8
+    // products are unrolled
+#pragma unroll 1
+    for (int r = 0; r < 8; ++r) {
+      double acc = 0.0;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) acc = acc + A[r + 8 * k] * x[k];
+      y[r] = acc;
+    }
+    return;
+  }
 #pragma unroll
   for (int r = 0; r < 8; ++r) {
     double acc = 0.0;
@@ -507,6 +572,13 @@ __device__ __forceinline__ void matvec8(const double* A, const double* x, double
     for (int k = 0; k < 8; ++k) acc = acc + A[r + 8 * k] * x[k];
     y[r] = acc;
   }
+}
+
+// eigenmatrix as one out-of-line copy, for the rolled limiter
+static __device__ __noinline__ void eigenmatrix_call(const Phys& P, int dir, double rho, double u1, double u2,
+                                                     double u3, double E, double B1, double B2, double B3,
+                                                     double* R, double* L) {
+  eigenmatrix(P, dir, rho, u1, u2, u3, E, B1, B2, B3, R, L);
 }
 
 __device__ __forceinline__ void trace8(const Consts& K, const double* __restrict__ S, long long c,
@@ -865,6 +937,7 @@ __device__ __forceinline__ void lim_tvb_p1(const Consts& K, const double* __rest
   word |= (int32_t)change;
 }
 
+template <bool ROLLED = false>
 __device__ __forceinline__ void lim_tvb(const Consts& K, const double* __restrict__ S, long long c,
                                         double (*m)[NP], int32_t& word) {
   if (K.tvb_p1) {
@@ -881,7 +954,8 @@ __device__ __forceinline__ void lim_tvb(const Consts& K, const double* __restric
     double Rp[NE], Rm[NE], Up[NE], Um[NE];
     unsigned change = 0;
     // x direction
-    eigenmatrix(K.P, 0, rhoij, u1, u2, u3, Eij, B1, B2, B3, R, L);
+    if (ROLLED) eigenmatrix_call(K.P, 0, rhoij, u1, u2, u3, Eij, B1, B2, B3, R, L);
+    else eigenmatrix(K.P, 0, rhoij, u1, u2, u3, Eij, B1, B2, B3, R, L);
 #pragma unroll
     for (int n = 0; n < NE; ++n) {
       DR[n] = S[c + 1 + pl * (10 * n)] - m[n][0];
@@ -889,24 +963,26 @@ __device__ __forceinline__ void lim_tvb(const Consts& K, const double* __restric
       Dp[n] = m[n][1] + c23 * m[n][3];
       Dm[n] = m[n][1] - c23 * m[n][3];
     }
-    matvec8(L, DR, t1);
-    matvec8(L, DL, t2);
-    matvec8(L, Dp, tu);
+    matvec8<ROLLED>(L, DR, t1);
+    matvec8<ROLLED>(L, DL, t2);
+    matvec8<ROLLED>(L, Dp, tu);
 #pragma unroll
     for (int k = 0; k < NE; ++k) mod[k] = minmod1(tu[k], t1[k], t2[k], K.Mh2x);
-    matvec8(R, mod, Rp);
+    matvec8<ROLLED>(R, mod, Rp);
 #pragma unroll
     for (int d = 0; d < NE; ++d)
       if (fabs(Rp[d] - Dp[d]) > 1e-6) change |= 1u << d;
-    matvec8(L, Dm, tu);
+    matvec8<ROLLED>(L, Dm, tu);
 #pragma unroll
     for (int k = 0; k < NE; ++k) mod[k] = minmod1(tu[k], t1[k], t2[k], K.Mh2x);
-    matvec8(R, mod, Rm);
+    matvec8<ROLLED>(R, mod, Rm);
 #pragma unroll
     for (int d = 0; d < NE; ++d)
       if (fabs(Rm[d] - Dm[d]) > 1e-6) change |= 1u << d;
     // y direction
-    if (K.eig_y_zero_w)
+    if (ROLLED)
+      eigenmatrix_call(K.P, 1, rhoij, u1, u2, K.eig_y_zero_w ? 0.0 : u3, Eij, B1, B2, K.eig_y_zero_w ? 0.0 : B3, R, L);
+    else if (K.eig_y_zero_w)
       eigenmatrix(K.P, 1, rhoij, u1, u2, 0.0, Eij, B1, B2, 0.0, R, L);
     else
       eigenmatrix(K.P, 1, rhoij, u1, u2, u3, Eij, B1, B2, B3, R, L);
@@ -917,19 +993,19 @@ __device__ __forceinline__ void lim_tvb(const Consts& K, const double* __restric
       Dp[n] = m[n][2] + c23 * m[n][5];
       Dm[n] = m[n][2] - c23 * m[n][5];
     }
-    matvec8(L, DR, t1);
-    matvec8(L, DL, t2);
-    matvec8(L, Dp, tu);
+    matvec8<ROLLED>(L, DR, t1);
+    matvec8<ROLLED>(L, DL, t2);
+    matvec8<ROLLED>(L, Dp, tu);
 #pragma unroll
     for (int k = 0; k < NE; ++k) mod[k] = minmod1(tu[k], t1[k], t2[k], K.Mh2y);
-    matvec8(R, mod, Up);
+    matvec8<ROLLED>(R, mod, Up);
 #pragma unroll
     for (int d = 0; d < NE; ++d)
       if (fabs(Up[d] - Dp[d]) > 1e-6) change |= 1u << d;
-    matvec8(L, Dm, tu);
+    matvec8<ROLLED>(L, Dm, tu);
 #pragma unroll
     for (int k = 0; k < NE; ++k) mod[k] = minmod1(tu[k], t1[k], t2[k], K.Mh2y);
-    matvec8(R, mod, Um);
+    matvec8<ROLLED>(R, mod, Um);
 #pragma unroll
     for (int d = 0; d < NE; ++d)
       if (fabs(Um[d] - Dm[d]) > 1e-6) change |= 1u << d;
@@ -1060,7 +1136,7 @@ __device__ __forceinline__ void limit_tvb_item(const Consts& K, const double* __
 #pragma unroll
     for (int d = 0; d < NP; ++d) m[n][d] = live_mode(n, d) ? S[c + pl * (d + 10 * n)] : 0.0;
   int32_t word = K.detector != GDF_DETECT_ALL ? (1 << 24) : 0;
-  lim_tvb(K, S, c, m, word);
+  lim_tvb<GDF_TVB_ROLLED>(K, S, c, m, word);
   lim_finish(K, D, BX, BY, flags, stage, divfree, sc, item, i, j, c, m, word);
 }
 

@@ -44,6 +44,11 @@
 #ifndef GDF_FACE_MINB
 #define GDF_FACE_MINB 4
 #endif
+// faces through the shared-memory staged kernel (k_face_tile) or one
+// thread per face point reading global memory (k_face); same values
+#ifndef GDF_FACE_STAGED
+#define GDF_FACE_STAGED 1
+#endif
 #ifndef GDF_CELL_MINB
 #define GDF_CELL_MINB 1
 #endif
@@ -73,6 +78,17 @@ __global__ void __launch_bounds__(128, GDF_FACE_MINB) k_face(const __grid_consta
   const long long item = gtid();
   if (item >= face_items<DIR>(K)) return;
   face_item<DIR>(K, U, Fh_out, Ez_out, item);
+}
+
+// The staged form of k_face: block (bx, by) takes faces bx*FACE_TILE ..
+// of face row by at all quadrature points.
+template <int DIR>
+__global__ void __launch_bounds__(128, GDF_FACE_MINB) k_face_tile(const __grid_constant__ Consts K,
+                                                    const double* __restrict__ U, double* __restrict__ Fh_out,
+                                                    double* __restrict__ Ez_out, const Scal* __restrict__ sc) {
+  __shared__ double ms[NLIVE][2 * FACE_TILE_W];
+  if (sc && !sc->active) return;
+  face_tile<DIR>(K, U, Fh_out, Ez_out, (int)blockIdx.x * FACE_TILE, (int)blockIdx.y, ms);
 }
 
 __global__ void __launch_bounds__(128, GDF_FACE_MINB) k_vertex(const __grid_constant__ Consts K, const double* __restrict__ U,
@@ -536,8 +552,15 @@ static int launch_faces(GdfHandle* h, const double* U, const Scal* sc) {
   const Consts& K = h->K;
   const long long nfx = (long long)(K.nx + 1) * NG * K.ny;
   const long long nfy = (long long)K.nx * NG * (K.ny + 1);
-  int rc = run_kernel(h, GDF_K_FACE_X, [&] { k_face<0><<<nblk(nfx, 128), 128, 0, h->st>>>(K, U, h->Fxh, h->EzRL, sc); });
-  if (!rc) rc = run_kernel(h, GDF_K_FACE_Y, [&] { k_face<1><<<nblk(nfy, 128), 128, 0, h->st>>>(K, U, h->Fyh, h->EzUD, sc); });
+  int rc;
+  if (GDF_FACE_STAGED && K.ny + 1 <= 65535) {
+    const dim3 gx((unsigned)nblk(K.nx + 1, FACE_TILE), (unsigned)K.ny), gy((unsigned)nblk(K.nx, FACE_TILE), (unsigned)(K.ny + 1));
+    rc = run_kernel(h, GDF_K_FACE_X, [&] { k_face_tile<0><<<gx, 128, 0, h->st>>>(K, U, h->Fxh, h->EzRL, sc); });
+    if (!rc) rc = run_kernel(h, GDF_K_FACE_Y, [&] { k_face_tile<1><<<gy, 128, 0, h->st>>>(K, U, h->Fyh, h->EzUD, sc); });
+  } else {
+    rc = run_kernel(h, GDF_K_FACE_X, [&] { k_face<0><<<nblk(nfx, 128), 128, 0, h->st>>>(K, U, h->Fxh, h->EzRL, sc); });
+    if (!rc) rc = run_kernel(h, GDF_K_FACE_Y, [&] { k_face<1><<<nblk(nfy, 128), 128, 0, h->st>>>(K, U, h->Fyh, h->EzUD, sc); });
+  }
   if (!rc) rc = run_kernel(h, GDF_K_VERTEX, [&] { k_vertex<<<nblk(K.vplane, 128), 128, 0, h->st>>>(K, U, h->EzV, sc); });
   return rc;
 }
