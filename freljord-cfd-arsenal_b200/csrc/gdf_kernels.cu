@@ -45,9 +45,10 @@
 #define GDF_FACE_MINB 4
 #endif
 // faces through the shared-memory staged kernel (k_face_tile) or one
-// thread per face point reading global memory (k_face); same values
+// thread per face point reading global memory (k_face, the default: the
+// staged form measured 30% slower, blast 2048^2, same values)
 #ifndef GDF_FACE_STAGED
-#define GDF_FACE_STAGED 1
+#define GDF_FACE_STAGED 0
 #endif
 #ifndef GDF_CELL_MINB
 #define GDF_CELL_MINB 1
