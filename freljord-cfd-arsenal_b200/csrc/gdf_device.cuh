@@ -104,10 +104,10 @@ __device__ __forceinline__ void face_point(const Consts& K, ML mL, MR mR, int g,
     uR[n] = b;
   }
   Side L, R;
-  make_side(K.P, uL, L);
-  make_side(K.P, uR, R);
+  make_side<true>(K.P, uL, L);
+  make_side<true>(K.P, uR, R);
   double Fh[NE], fL[NE], fR[NE];
-  face_flux_sides(K.P, L, R, DIR, Fh, fL, fR);
+  face_flux_sides<true>(K.P, L, R, DIR, Fh, fL, fR);
   const long long fp = DIR == 0 ? K.fxplane : K.fyplane;
 #pragma unroll
   for (int n = 0; n < NE; ++n) Fh_out[(n * NG + g) * fp + o] = Fh[n];
@@ -255,7 +255,7 @@ __device__ __forceinline__ void cell_item(const Consts& K, const double* __restr
           v[n] = acc;
         }
         const double rho = v[0];
-        const double u = dv(v[1], rho), vv = dv(v[2], rho), w = dv(v[3], rho);
+        const double u = v[1] / rho, vv = v[2] / rho, w = dv(v[3], rho);   // rho w = 0 in 2-D runs
         const double E = v[4], B1 = v[5], B2 = v[6], B3 = v[7];
         const double BB = sq(B1) + sq(B2) + sq(B3);
         const double p = K.P.gamma1 * (E - 0.5 * rho * (sq(u) + sq(vv) + sq(w)) - 0.5 * BB);
@@ -328,7 +328,7 @@ __device__ __forceinline__ void cell_item(const Consts& K, const double* __restr
           if (g == 2 && (d == 1 || d == 4 || d == 8 || d == 6)) continue;
           acc = acc - K.cys * c_basis.w[g] * (fu[g] * c_basis.phiGU[g][d] - fd[g] * c_basis.phiGD[g][d]);
         }
-        du[LI(n, d)] = dv(acc, c_basis.mm[d]);
+        du[LI(n, d)] = (n == 3 || n == 7) ? dv(acc, c_basis.mm[d]) : acc / c_basis.mm[d];
       }
     }
   }
@@ -390,7 +390,7 @@ __device__ __forceinline__ void bface_item(const Consts& K, const double* __rest
       double acc = 0.0;
 #pragma unroll
       for (int g = 0; g < NG; ++g) acc = acc + 0.5 * c_basis.w[g] * EzRL[g * fp + o] * K.EzyG[g][d];
-      dez[d] = dv(acc - dv(v1 * c_basis.EzU[d], K.hy) + dv(v0 * c_basis.EzD[d], K.hy), c_basis.mmE[d]);
+      dez[d] = (acc - v1 * c_basis.EzU[d] / K.hy + v0 * c_basis.EzD[d] / K.hy) / c_basis.mmE[d];
     }
     B = BX; B0 = BX0; BI = BXI; dout = dez1;
   } else {
@@ -406,7 +406,7 @@ __device__ __forceinline__ void bface_item(const Consts& K, const double* __rest
       double acc = 0.0;
 #pragma unroll
       for (int g = 0; g < NG; ++g) acc = acc - 0.5 * c_basis.w[g] * EzUD[g * fp + o] * K.EzxG[g][d];
-      dez[d] = dv(acc + dv(v1 * c_basis.EzR[d], K.hx) - dv(v0 * c_basis.EzL[d], K.hx), c_basis.mmE[d]);
+      dez[d] = (acc + v1 * c_basis.EzR[d] / K.hx - v0 * c_basis.EzL[d] / K.hx) / c_basis.mmE[d];
     }
     B = BY; B0 = BY0; BI = BYI; dout = dez2;
   }
@@ -890,7 +890,7 @@ __device__ __forceinline__ void lim_tvb_p1(const Consts& K, const double* __rest
                                            double (*m)[NP], int32_t& word) {
   const long long pl = K.plane;
   const double rhoij = m[0][0];
-  const double u1 = dv(m[1][0], rhoij), u2 = dv(m[2][0], rhoij), u3 = dv(m[3][0], rhoij);
+  const double u1 = m[1][0] / rhoij, u2 = m[2][0] / rhoij, u3 = dv(m[3][0], rhoij);
   const double Eij = m[4][0], B1 = m[5][0], B2 = m[6][0], B3 = m[7][0];
   double R[64], L[64];
   double DR[NE], DL[NE], D1[NE], t1[NE], t2[NE], tu[NE], mod[NE], Xm[NE], Ym[NE];
@@ -949,7 +949,7 @@ __device__ __forceinline__ void lim_tvb(const Consts& K, const double* __restric
   const long long pl = K.plane;
     const double c23 = 2.0 / 3.0;
     const double rhoij = m[0][0];
-    const double u1 = dv(m[1][0], rhoij), u2 = dv(m[2][0], rhoij), u3 = dv(m[3][0], rhoij);
+    const double u1 = m[1][0] / rhoij, u2 = m[2][0] / rhoij, u3 = dv(m[3][0], rhoij);
     const double Eij = m[4][0], B1 = m[5][0], B2 = m[6][0], B3 = m[7][0];
     double R[64], L[64];
     double DR[NE], DL[NE], Dp[NE], Dm[NE], t1[NE], t2[NE], tu[NE], mod[NE];

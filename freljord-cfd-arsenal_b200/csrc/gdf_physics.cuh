@@ -64,6 +64,17 @@ GDF_HD double sqrt0(double x) {
 #endif
   return sqrt(x);
 }
+// The face solvers take the shortcut (ZF); elsewhere the plain operation
+// measured faster (the vertex solver and the limiter's eigenvectors meet
+// few exact zeros and their code grows with the extra test).
+template <bool ZF>
+GDF_HD double dvz(double x, double y) {
+  return ZF ? dv(x, y) : x / y;
+}
+template <bool ZF>
+GDF_HD double sqz(double x) {
+  return ZF ? sqrt0(x) : sqrt(x);
+}
 
 // Run-time physics constants shared by every kernel.
 struct Phys {
@@ -86,13 +97,14 @@ struct Side {
   double rho, u, v, w, E, B1, B2, B3, BB, p;
 };
 
+template <bool ZF = false>
 GDF_HD void make_side(const Phys& P, const double* U, Side& s) {
 #pragma unroll
   for (int n = 0; n < NE; ++n) s.U[n] = U[n];
   s.rho = U[0];
-  s.u = dv(U[1], s.rho);
-  s.v = dv(U[2], s.rho);
-  s.w = dv(U[3], s.rho);
+  s.u = dvz<ZF>(U[1], s.rho);
+  s.v = dvz<ZF>(U[2], s.rho);
+  s.w = dvz<ZF>(U[3], s.rho);
   s.E = U[4];
   s.B1 = U[5];
   s.B2 = U[6];
@@ -159,14 +171,15 @@ GDF_HD void side_flux_hard(const Phys& P, const Side& s, double* Fx, double* Fy)
 }
 
 // eigenvalueMm.f90 from a state's primitives (normal x: dir 0, y: dir 1)
+template <bool ZF = false>
 GDF_HD void side_speeds(const Phys& P, const Side& s, int dir, double& amax, double& amin) {
   const double Bn = dir == 0 ? s.B1 : s.B2;
   const double un = dir == 0 ? s.u : s.v;
-  const double c = sqrt0(fabs(dv(P.gamma * s.p, s.rho)));
+  const double c = sqz<ZF>(fabs(dvz<ZF>(P.gamma * s.p, s.rho)));
   const double c2 = sq(c);
-  const double br = dv(s.BB, s.rho);
+  const double br = dvz<ZF>(s.BB, s.rho);
   const double X = c2 + br;
-  const double cf = sqrt0(fabs(0.5 * (c2 + br + sqrt0(sq(X) - dv(4 * c2 * sq(Bn), s.rho)))));
+  const double cf = sqz<ZF>(fabs(0.5 * (c2 + br + sqz<ZF>(sq(X) - dvz<ZF>(4 * c2 * sq(Bn), s.rho)))));
   amax = un + cf;
   amin = un - cf;
 }
@@ -175,16 +188,16 @@ GDF_HD void side_speeds(const Phys& P, const Side& s, int dir, double& amax, dou
 // eigenvalueMm.f90:1-25 for the normal (1,0) (dir 0) or (0,1) (dir 1).
 GDF_HD void fast_speeds(const Phys& P, const double* U, int dir, double& amax, double& amin) {
   const double rho = U[0];
-  const double u = dv(U[1], rho), v = dv(U[2], rho), w = dv(U[3], rho);
+  const double u = dvz<false>(U[1], rho), v = dvz<false>(U[2], rho), w = dvz<false>(U[3], rho);
   const double B1 = U[5], B2 = U[6], B3 = U[7];
   const double BP = sq(B1) + sq(B2) + sq(B3);
   const double Bn = dir == 0 ? B1 : B2;
   const double un = dir == 0 ? u : v;
   const double p = P.gamma1 * (U[4] - 0.5 * rho * (sq(u) + sq(v) + sq(w)) - 0.5 * BP);
-  const double c = sqrt0(fabs(dv(P.gamma * p, rho)));
+  const double c = sqz<false>(fabs(dvz<false>(P.gamma * p, rho)));
   const double c2 = sq(c);
-  const double X = c2 + dv(BP, rho);
-  const double cf = sqrt0(fabs(0.5 * (c2 + dv(BP, rho) + sqrt0(sq(X) - dv(4 * c2 * sq(Bn), rho)))));
+  const double X = c2 + dvz<false>(BP, rho);
+  const double cf = sqz<false>(fabs(0.5 * (c2 + dvz<false>(BP, rho) + sqz<false>(sq(X) - dvz<false>(4 * c2 * sq(Bn), rho)))));
   amax = un + cf;
   amin = un - cf;
 }
@@ -193,7 +206,7 @@ GDF_HD void fast_speeds(const Phys& P, const double* U, int dir, double& amax, d
 // HLLC_Flux.f90:9-106 and HLLD_Flux.f90:14-189 share the first stage.
 // dir 0 = normal x (reference direction 1), 1 = normal y (direction 2).
 // Fh gets the flux, Ust the star state (Ustar of the reference).
-template <bool HLLD>
+template <bool HLLD, bool ZF = false>
 GDF_HD void hllcd_flux(const Phys& P, const Side& R, const Side& L, const double* FR, const double* FL, double SR,
                        double SL, int dir, double* Fh, double* Ust) {
   if (SR < 0) {
@@ -210,19 +223,19 @@ GDF_HD void hllcd_flux(const Phys& P, const Side& R, const Side& L, const double
   const double* UL1 = L.U;
   double Us[NE];
 #pragma unroll
-  for (int n = 0; n < NE; ++n) Us[n] = dv(SR * UR1[n] - SL * UL1[n] + FL[n] - FR[n], SR - SL);
+  for (int n = 0; n < NE; ++n) Us[n] = dvz<ZF>(SR * UR1[n] - SL * UL1[n] + FL[n] - FR[n], SR - SL);
   const double rhoR = R.rho, u1R = R.u, u2R = R.v, u3R = R.w, ER = R.E;
   const double B1R = R.B1, B2R = R.B2, B3R = R.B3;
   const double rhoL = L.rho, u1L = L.u, u2L = L.v, u3L = L.w, EL = L.E;
   const double B1L = L.B1, B2L = L.B2, B3L = L.B3;
-  const double Sstar = dv(dir == 0 ? Us[1] : Us[2], Us[0]);
+  const double Sstar = dvz<ZF>(dir == 0 ? Us[1] : Us[2], Us[0]);
   const double uRbot = dir == 0 ? u1R : u2R, uLbot = dir == 0 ? u1L : u2L;
   const double BRbot = dir == 0 ? B1R : B2R, BLbot = dir == 0 ? B1L : B2L;
   const double Bsb = dir == 0 ? Us[5] : Us[6];
   const double dR = SR - uRbot, dL = SL - uLbot;      // (SR - uRbot), (SL - uLbot)
   const double eR = SR - Sstar, eL = SL - Sstar;      // (SR - Sstar), (SL - Sstar)
-  const double rhoRs = dv(rhoR * dR, eR);
-  const double rhoLs = dv(rhoL * dL, eL);
+  const double rhoRs = dvz<ZF>(rhoR * dR, eR);
+  const double rhoLs = dvz<ZF>(rhoL * dL, eL);
   const double PtotR = P.gamma1 * (ER - 0.5 * rhoR * (sq(u1R) + sq(u2R) + sq(u3R)));
   const double PtotL = P.gamma1 * (EL - 0.5 * rhoL * (sq(u1L) + sq(u2L) + sq(u3L)));
   const double PtotRs = PtotR + rhoR * dR * (Sstar - uRbot) + sq(Bsb) - sq(BRbot);
@@ -230,8 +243,8 @@ GDF_HD void hllcd_flux(const Phys& P, const Side& R, const Side& L, const double
   double B1Rs, B1Ls, B2Rs, B2Ls, B3Rs, B3Ls;
   double SRs = 0, SLs = 0;
   if (HLLD) {
-    SRs = Sstar + sqrt0(dv(sq(Bsb), rhoRs));
-    SLs = Sstar - sqrt0(dv(sq(Bsb), rhoLs));
+    SRs = Sstar + sqz<ZF>(dvz<ZF>(sq(Bsb), rhoRs));
+    SLs = Sstar - sqz<ZF>(dvz<ZF>(sq(Bsb), rhoLs));
     const double AR = rhoR * sq(dR) - Bsb * BRbot;
     const double AL = rhoL * sq(dL) - Bsb * BLbot;
     const double CR = rhoR * dR * (BRbot - Bsb);
@@ -240,37 +253,37 @@ GDF_HD void hllcd_flux(const Phys& P, const Side& R, const Side& L, const double
     const double DL = rhoL * dL * eL - sq(Bsb) + 1e-15;
     if (dir == 0) {
       B1Rs = Bsb; B1Ls = Bsb;
-      B2Rs = dv(AR * B2R + CR * u2R, DR);
-      B2Ls = dv(AL * B2L + CL * u2L, DL);
+      B2Rs = dvz<ZF>(AR * B2R + CR * u2R, DR);
+      B2Ls = dvz<ZF>(AL * B2L + CL * u2L, DL);
     } else {
-      B1Rs = dv(AR * B1R + CR * u1R, DR);
-      B1Ls = dv(AL * B1L + CL * u1L, DL);
+      B1Rs = dvz<ZF>(AR * B1R + CR * u1R, DR);
+      B1Ls = dvz<ZF>(AL * B1L + CL * u1L, DL);
       B2Rs = Bsb; B2Ls = Bsb;
     }
-    B3Rs = dv(AR * B3R + CR * u3R, DR);
-    B3Ls = dv(AL * B3L + CL * u3L, DL);
+    B3Rs = dvz<ZF>(AR * B3R + CR * u3R, DR);
+    B3Ls = dvz<ZF>(AL * B3L + CL * u3L, DL);
   } else {
     B1Rs = Us[5]; B1Ls = Us[5]; B2Rs = Us[6]; B2Ls = Us[6]; B3Rs = Us[7]; B3Ls = Us[7];
   }
   double URs[NE], ULs[NE];
   if (dir == 0) {
-    URs[1] = dv(UR1[1] * dR + PtotRs - PtotR + BRbot * B1R - Bsb * B1Rs, eR);
-    URs[2] = dv(UR1[2] * dR + BRbot * B2R - Bsb * B2Rs, eR);
-    ULs[1] = dv(UL1[1] * dL + PtotLs - PtotL + BLbot * B1L - Bsb * B1Ls, eL);
-    ULs[2] = dv(UL1[2] * dL + BLbot * B2L - Bsb * B2Ls, eL);
+    URs[1] = dvz<ZF>(UR1[1] * dR + PtotRs - PtotR + BRbot * B1R - Bsb * B1Rs, eR);
+    URs[2] = dvz<ZF>(UR1[2] * dR + BRbot * B2R - Bsb * B2Rs, eR);
+    ULs[1] = dvz<ZF>(UL1[1] * dL + PtotLs - PtotL + BLbot * B1L - Bsb * B1Ls, eL);
+    ULs[2] = dvz<ZF>(UL1[2] * dL + BLbot * B2L - Bsb * B2Ls, eL);
   } else {
-    URs[1] = dv(UR1[1] * dR + BRbot * B1R - Bsb * B1Rs, eR);
-    URs[2] = dv(UR1[2] * dR + PtotRs - PtotR + BRbot * B2R - Bsb * B2Rs, eR);
-    ULs[1] = dv(UL1[1] * dL + BLbot * B1L - Bsb * B1Ls, eL);
-    ULs[2] = dv(UL1[2] * dL + PtotLs - PtotL + BLbot * B2L - Bsb * B2Ls, eL);
+    URs[1] = dvz<ZF>(UR1[1] * dR + BRbot * B1R - Bsb * B1Rs, eR);
+    URs[2] = dvz<ZF>(UR1[2] * dR + PtotRs - PtotR + BRbot * B2R - Bsb * B2Rs, eR);
+    ULs[1] = dvz<ZF>(UL1[1] * dL + BLbot * B1L - Bsb * B1Ls, eL);
+    ULs[2] = dvz<ZF>(UL1[2] * dL + PtotLs - PtotL + BLbot * B2L - Bsb * B2Ls, eL);
   }
-  URs[3] = dv(UR1[3] * dR + BRbot * B3R - Bsb * B3Rs, eR);
-  ULs[3] = dv(UL1[3] * dL + BLbot * B3L - Bsb * B3Ls, eL);
-  const double u1Rs = dv(URs[1], rhoRs), u2Rs = dv(URs[2], rhoRs), u3Rs = dv(URs[3], rhoRs);
-  const double u1Ls = dv(ULs[1], rhoLs), u2Ls = dv(ULs[2], rhoLs), u3Ls = dv(ULs[3], rhoLs);
-  const double ERs = dv(dR * ER - PtotR * uRbot + PtotRs * Sstar + BRbot * (u1R * B1R + u2R * B2R + u3R * B3R) -
+  URs[3] = dvz<ZF>(UR1[3] * dR + BRbot * B3R - Bsb * B3Rs, eR);
+  ULs[3] = dvz<ZF>(UL1[3] * dL + BLbot * B3L - Bsb * B3Ls, eL);
+  const double u1Rs = dvz<ZF>(URs[1], rhoRs), u2Rs = dvz<ZF>(URs[2], rhoRs), u3Rs = dvz<ZF>(URs[3], rhoRs);
+  const double u1Ls = dvz<ZF>(ULs[1], rhoLs), u2Ls = dvz<ZF>(ULs[2], rhoLs), u3Ls = dvz<ZF>(ULs[3], rhoLs);
+  const double ERs = dvz<ZF>(dR * ER - PtotR * uRbot + PtotRs * Sstar + BRbot * (u1R * B1R + u2R * B2R + u3R * B3R) -
                             Bsb * (u1Rs * B1Rs + u2Rs * B2Rs + u3Rs * B3Rs), eR);
-  const double ELs = dv(dL * EL - PtotL * uLbot + PtotLs * Sstar + BLbot * (u1L * B1L + u2L * B2L + u3L * B3L) -
+  const double ELs = dvz<ZF>(dL * EL - PtotL * uLbot + PtotLs * Sstar + BLbot * (u1L * B1L + u2L * B2L + u3L * B3L) -
                             Bsb * (u1Ls * B1Ls + u2Ls * B2Ls + u3Ls * B3Ls), eL);
   URs[0] = rhoRs; URs[4] = ERs;
   ULs[0] = rhoLs; ULs[4] = ELs;
@@ -289,13 +302,13 @@ GDF_HD void hllcd_flux(const Phys& P, const Side& R, const Side& L, const double
       const double sL = sqrt(fabs(rhoLs)), sR = sqrt(fabs(rhoRs));
       const double sg = sgn1(Bsb);
       const double den = sL + sR;
-      const double u1ss = dv(sL * u1Ls + sR * u1Rs + sg * (B1Rs - B1Ls), den);
-      const double u2ss = dv(sL * u2Ls + sR * u2Rs + sg * (B2Rs - B2Ls), den);
-      const double u3ss = dv(sL * u3Ls + sR * u3Rs + sg * (B3Rs - B3Ls), den);
+      const double u1ss = dvz<ZF>(sL * u1Ls + sR * u1Rs + sg * (B1Rs - B1Ls), den);
+      const double u2ss = dvz<ZF>(sL * u2Ls + sR * u2Rs + sg * (B2Rs - B2Ls), den);
+      const double u3ss = dvz<ZF>(sL * u3Ls + sR * u3Rs + sg * (B3Rs - B3Ls), den);
       const double sLR = sqrt(fabs(rhoLs * rhoRs));
-      const double B1ss = dv(sL * B1Ls + sR * B1Rs + sg * sLR * (u1Rs - u1Ls), den);
-      const double B2ss = dv(sL * B2Ls + sR * B2Rs + sg * sLR * (u2Rs - u2Ls), den);
-      const double B3ss = dv(sL * B3Ls + sR * B3Rs + sg * sLR * (u3Rs - u3Ls), den);
+      const double B1ss = dvz<ZF>(sL * B1Ls + sR * B1Rs + sg * sLR * (u1Rs - u1Ls), den);
+      const double B2ss = dvz<ZF>(sL * B2Ls + sR * B2Rs + sg * sLR * (u2Rs - u2Ls), den);
+      const double B3ss = dvz<ZF>(sL * B3Ls + sR * B3Rs + sg * sLR * (u3Rs - u3Ls), den);
       if (Sstar > 0) {
         const double ELss = ELs - sL * (u1Ls * B1Ls + u2Ls * B2Ls + u3Ls * B3Ls - u1ss * B1ss - u2ss * B2ss -
                                         u3ss * B3ss) * sg;
@@ -333,6 +346,7 @@ GDF_HD void hllcd_flux(const Phys& P, const Side& R, const Side& L, const double
 // reference's UL1), uR = +normal side (UR1); dir 0 = x, 1 = y. Writes the
 // numerical flux Fh and returns the fluxes of both sides in fL / fR and the
 // normal velocities of both sides in unL / unR (used by the face Ez).
+template <bool ZF = false>
 GDF_HD void face_flux_sides(const Phys& P, const Side& L, const Side& R, int dir, double* Fh, double* fL,
                             double* fR) {
   if (dir == 0) {
@@ -343,8 +357,8 @@ GDF_HD void face_flux_sides(const Phys& P, const Side& L, const Side& R, int dir
     side_flux_y(P, R, fR, true);
   }
   double a1, a2, b1, b2;
-  side_speeds(P, L, dir, a1, a2);   // SRmax/SRmin of the reference (from UR(i) = left side)
-  side_speeds(P, R, dir, b1, b2);   // SLmax/SLmin (from UL(i+1) = right side)
+  side_speeds<ZF>(P, L, dir, a1, a2);   // SRmax/SRmin of the reference (from UR(i) = left side)
+  side_speeds<ZF>(P, R, dir, b1, b2);   // SLmax/SLmin (from UL(i+1) = right side)
   const double SR = fmax2(a1, b1);
   const double SL = fmin2(a2, b2);
   double Ust[NE];
@@ -362,12 +376,12 @@ GDF_HD void face_flux_sides(const Phys& P, const Side& L, const Side& R, int dir
     } else {
       const double den = SR - SL, sls = SL * SR;
 #pragma unroll
-      for (int n = 0; n < NE; ++n) Fh[n] = dv(SR * fL[n] - SL * fR[n] + sls * (R.U[n] - L.U[n]), den);
+      for (int n = 0; n < NE; ++n) Fh[n] = dvz<ZF>(SR * fL[n] - SL * fR[n] + sls * (R.U[n] - L.U[n]), den);
     }
   } else if (P.flux == 3) {
-    hllcd_flux<false>(P, R, L, fR, fL, SR, SL, dir, Fh, Ust);
+    hllcd_flux<false, ZF>(P, R, L, fR, fL, SR, SL, dir, Fh, Ust);
   } else {
-    hllcd_flux<true>(P, R, L, fR, fL, SR, SL, dir, Fh, Ust);
+    hllcd_flux<true, ZF>(P, R, L, fR, fL, SR, SL, dir, Fh, Ust);
   }
 }
 
@@ -389,8 +403,8 @@ GDF_HD void hll1_cm(const double* UR, const double* UL, const double* FR, const 
   } else if (SL > 0) {
     uk = UL[k]; fm = FL[m];
   } else {
-    fm = dv(SR * FL[m] - SL * FR[m] + SL * SR * (UR[m] - UL[m]), SR - SL);
-    uk = dv(SR * UR[k] - SL * UL[k] - (FR[k] - FL[k]), SR - SL);
+    fm = dvz<false>(SR * FL[m] - SL * FR[m] + SL * SR * (UR[m] - UL[m]), SR - SL);
+    uk = dvz<false>(SR * UR[k] - SL * UL[k] - (FR[k] - FL[k]), SR - SL);
   }
 }
 
@@ -452,9 +466,9 @@ GDF_HD double vertex_ez(const Phys& P, const double* URU, const double* ULU, con
     const double BxRU = URU[5], BxLU = ULU[5], BxRD = URD[5], BxLD = ULD[5];
     const double ByRU = URU[6], ByLU = ULU[6], ByRD = URD[6], ByLD = ULD[6];
     const double den = 2 * (SR - SL) * (SU - SD);
-    const double BxSS = dv(2 * SR * SU * BxRU - 2 * SL * SU * BxLU + 2 * SL * SD * BxLD - 2 * SR * SD * BxRD -
+    const double BxSS = dvz<false>(2 * SR * SU * BxRU - 2 * SL * SU * BxLU + 2 * SL * SD * BxLD - 2 * SR * SD * BxRD -
                                SR * (z - z) + SL * (z - z) - (SR - SL) * (EzUs - EzDs), den);
-    const double BySS = dv(2 * SR * SU * ByRU - 2 * SL * SU * ByLU + 2 * SL * SD * ByLD - 2 * SR * SD * ByRD +
+    const double BySS = dvz<false>(2 * SR * SU * ByRU - 2 * SL * SU * ByLU + 2 * SL * SD * ByLD - 2 * SR * SD * ByRD +
                                SU * (z - z) - SD * (z - z) + (SU - SD) * (EzRs - EzLs), den);
     return 0.25 * (EzRs + EzLs + EzUs + EzDs) - 0.25 * SU * (BxUs - BxSS) - 0.25 * SD * (BxDs - BxSS) +
            0.25 * SR * (ByRs - BySS) + 0.25 * SL * (ByLs - BySS);
@@ -529,12 +543,12 @@ GDF_HD void eigenmatrix(const Phys& P, int dir, double rho, double u1, double u2
     const double sqpr = sqrt(fabs(p)) / rho;
     const double sqpor = sqrt(fabs(p / rho));
     const double sq1og = sqrt(1.0 / gm);
-    const double b1s = dv(B1, rhosq), b2s = dv(B2, rhosq), b3s = dv(B3, rhosq);
+    const double b1s = dvz<false>(B1, rhosq), b2s = dvz<false>(B2, rhosq), b3s = dvz<false>(B3, rhosq);
     const double bN = dir == 0 ? b1s : b2s;
     const double d = a2 + (sq(b1s) + sq(b2s) + sq(b3s));
     const double disc = sqrt(fabs(sq(d) - 4.0 * a2 * sq(bN)));
-    const double cf = sqrt0(0.5 * fabs(d + disc));
-    const double cs = sqrt0(0.5 * fabs(d - disc));
+    const double cf = sqz<false>(0.5 * fabs(d + disc));
+    const double cs = sqz<false>(0.5 * fabs(d - disc));
     const double bNsum = dir == 0 ? ((b1s + b2s * 0.0) + b3s * 0.0) : ((b1s * 0.0 + b2s) + b3s * 0.0);
     const double beta1 = sgn1(bNsum * 1.0);
     double alphaf, alphas;
@@ -542,9 +556,9 @@ GDF_HD void eigenmatrix(const Phys& P, int dir, double rho, double u1, double u2
       alphaf = 0x1.6a09e667f3bccp-1;
       alphas = 0x1.6a09e667f3bcdp-1;
     } else {
-      const double den = sqrt0(fabs(cf * cf - cs * cs));
-      alphaf = dv(sqrt0(fabs(a2 - cs * cs)), den);
-      alphas = dv(sqrt0(fabs(cf * cf - a2)), den);
+      const double den = sqz<false>(fabs(cf * cf - cs * cs));
+      alphaf = dvz<false>(sqz<false>(fabs(a2 - cs * cs)), den);
+      alphas = dvz<false>(sqz<false>(fabs(cf * cf - a2)), den);
     }
     const double bst = (b1s * t1 + b2s * t2 + b3s * t3);
     const double rc = rhosq * cf;
@@ -569,9 +583,9 @@ GDF_HD void eigenmatrix(const Phys& P, int dir, double rho, double u1, double u2
       const double m1 = dir == 0 ? (afa2 + asa * (bst - bN * t1)) : (asa * (-(bN * t1)));
       const double m2 = dir == 1 ? (afa2 + asa * (bst - bN * t2)) : (asa * (-(bN * t2)));
       const double m3 = asa * (-(bN * t3));
-      ru[1][4] = dv(sqg2 * m1, rc);
-      ru[2][4] = dv(sqg2 * m2, rc);
-      ru[3][4] = dv(sqg2 * m3, rc);
+      ru[1][4] = dvz<false>(sqg2 * m1, rc);
+      ru[2][4] = dvz<false>(sqg2 * m2, rc);
+      ru[3][4] = dvz<false>(sqg2 * m3, rc);
     }
     ru[0][4] = sqg2 * alphaf * rhosq;
     ru[4][4] = sqg2 * alphaf * rhosq * a2;
@@ -585,9 +599,9 @@ GDF_HD void eigenmatrix(const Phys& P, int dir, double rho, double u1, double u2
       const double k1 = dir == 0 ? (alphaf * cf2 * t1 + a * alphas * bN) : (alphaf * cf2 * t1);
       const double k2 = dir == 1 ? (alphaf * cf2 * t2 + alphas * a * bN) : (alphaf * cf2 * t2);
       const double k3 = alphaf * cf2 * t3;
-      ru[1][6] = dv(bs * k1, rc);
-      ru[2][6] = dv(bs * k2, rc);
-      ru[3][6] = dv(bs * k3, rc);
+      ru[1][6] = dvz<false>(bs * k1, rc);
+      ru[2][6] = dvz<false>(bs * k2, rc);
+      ru[3][6] = dvz<false>(bs * k3, rc);
     }
     ru[0][6] = sqg2 * alphas * rhosq;
     ru[4][6] = sq(a) * sqg2 * alphas * rhosq;
@@ -609,15 +623,15 @@ GDF_HD void eigenmatrix(const Phys& P, int dir, double rho, double u1, double u2
     const double k2 = sq(u1) + sq(u2) + sq(u3);
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
-      R[0 + 8 * m] = dv(ru[0][m], g1);
-      R[1 + 8 * m] = dv(ru[0][m] * u1 + ru[1][m] * rho, g1);
-      R[2 + 8 * m] = dv(ru[0][m] * u2 + ru[2][m] * rho, g1);
-      R[3 + 8 * m] = dv(ru[0][m] * u3 + ru[3][m] * rho, g1);
-      R[4 + 8 * m] = dv(dv(ru[4][m], g1) + B1 * ru[5][m] + B2 * ru[6][m] + B3 * ru[7][m] + 0.5 * ru[0][m] * k2 +
+      R[0 + 8 * m] = dvz<false>(ru[0][m], g1);
+      R[1 + 8 * m] = dvz<false>(ru[0][m] * u1 + ru[1][m] * rho, g1);
+      R[2 + 8 * m] = dvz<false>(ru[0][m] * u2 + ru[2][m] * rho, g1);
+      R[3 + 8 * m] = dvz<false>(ru[0][m] * u3 + ru[3][m] * rho, g1);
+      R[4 + 8 * m] = dvz<false>(dvz<false>(ru[4][m], g1) + B1 * ru[5][m] + B2 * ru[6][m] + B3 * ru[7][m] + 0.5 * ru[0][m] * k2 +
                             ru[1][m] * u1 * rho + ru[2][m] * u2 * rho + ru[3][m] * u3 * rho, g1);
-      R[5 + 8 * m] = dv(ru[5][m], g1);
-      R[6 + 8 * m] = dv(ru[6][m], g1);
-      R[7 + 8 * m] = dv(ru[7][m], g1);
+      R[5 + 8 * m] = dvz<false>(ru[5][m], g1);
+      R[6 + 8 * m] = dvz<false>(ru[6][m], g1);
+      R[7 + 8 * m] = dvz<false>(ru[7][m], g1);
     }
   }
 
@@ -626,21 +640,21 @@ GDF_HD void eigenmatrix(const Phys& P, int dir, double rho, double u1, double u2
     const double rhosq = sqrt(rho);
     const double a2 = fabs(gm * p / rho);
     const double a = sqrt(a2);
-    const double b1s = dv(B1, rhosq), b2s = dv(B2, rhosq), b3s = dv(B3, rhosq);
+    const double b1s = dvz<false>(B1, rhosq), b2s = dvz<false>(B2, rhosq), b3s = dvz<false>(B3, rhosq);
     const double BNs = dir == 0 ? b1s : b2s;
     const double BN = dir == 0 ? B1 : B2;
     const double d = a2 + (sq(b1s) + sq(b2s) + sq(b3s));
     const double disc = sqrt(fabs(sq(d) - 4.0 * a2 * sq(BNs)));
-    const double cf = sqrt0(0.5 * fabs(d + disc));
-    const double cs = sqrt0(0.5 * fabs(d - disc));
+    const double cf = sqz<false>(0.5 * fabs(d + disc));
+    const double cs = sqz<false>(0.5 * fabs(d - disc));
     double alphaf, alphas;
     if (fabs(cf * cf - cs * cs) <= 1.0e-12) {
       alphaf = 0x1.6a09e667f3bccp-1;
       alphas = 0x1.6a09e667f3bcdp-1;
     } else {
-      const double den = sqrt0(fabs(cf * cf - cs * cs));
-      alphaf = dv(sqrt0(fabs(a2 - cs * cs)), den);
-      alphas = dv(sqrt0(fabs(cf * cf - a2)), den);
+      const double den = sqz<false>(fabs(cf * cf - cs * cs));
+      alphaf = dvz<false>(sqz<false>(fabs(a2 - cs * cs)), den);
+      alphas = dvz<false>(sqz<false>(fabs(cf * cf - a2)), den);
     }
     const double twosq = sqrt(2.0);
     // sign(1, BNs*1): BNs summed as (b1s*n1 + b2s*n2) + b3s*n3 so that the
@@ -661,30 +675,30 @@ GDF_HD void eigenmatrix(const Phys& P, int dir, double rho, double u1, double u2
     const double nen = dir == 0 ? (sq(t2) + sq(t3)) : (sq(t1) + sq(t3));
     const double nen2 = a * gu1sq * nen;
     if (dir == 0) {
-      lu[1][5] = dv(sq(t2) + sq(t3), nen2);
-      lu[1][6] = dv(-(t2 * t1), nen2);
-      lu[1][7] = dv(-(t1 * t3), nen2);
+      lu[1][5] = dvz<false>(sq(t2) + sq(t3), nen2);
+      lu[1][6] = dvz<false>(-(t2 * t1), nen2);
+      lu[1][7] = dvz<false>(-(t1 * t3), nen2);
     } else {
-      lu[1][5] = dv(-(t1 * t2), nen2);
-      lu[1][6] = dv(sq(t1) + sq(t3), nen2);
-      lu[1][7] = dv(-(t2 * t3), nen2);
+      lu[1][5] = dvz<false>(-(t1 * t2), nen2);
+      lu[1][6] = dvz<false>(sq(t1) + sq(t3), nen2);
+      lu[1][7] = dvz<false>(-(t2 * t3), nen2);
     }
     const double nen3 = sqrt(2.0) * sqrt(fabs(p)) * nen;
     const double nen31 = nen3 / sqrt(fabs(rho));
-    lu[2][1] = dv(rho * (-TxN1), nen3);
-    lu[2][2] = dv(rho * (-TxN2), nen3);
-    lu[2][3] = dv(rho * (-TxN3), nen3);
-    lu[2][5] = dv(TxN1, nen31);
-    lu[2][6] = dv(TxN2, nen31);
-    lu[2][7] = dv(TxN3, nen31);
+    lu[2][1] = dvz<false>(rho * (-TxN1), nen3);
+    lu[2][2] = dvz<false>(rho * (-TxN2), nen3);
+    lu[2][3] = dvz<false>(rho * (-TxN3), nen3);
+    lu[2][5] = dvz<false>(TxN1, nen31);
+    lu[2][6] = dvz<false>(TxN2, nen31);
+    lu[2][7] = dvz<false>(TxN3, nen31);
     const double cf2 = sq(cf);
     const double q = a * sq(BN) * sq(alphas) + rhosq * cf2 * alphaf * (a * rhosq * alphaf + BT * alphas);
     const double nen51 = twosq * a * nen * gu1sq * q;
     const double nen52 = twosq * a * gu1sq * (sq(alphaf) + sq(alphas)) * nen;
     const double nen71 = twosq * beta1 * nen * gu1sq * q;
     const double rcf = rho * cf;
-    const double Term54 = dv(alphaf, twosq * sq(a) * gu1sq * rhosq * (sq(alphaf) + sq(alphas)));
-    const double Term74 = dv(alphas, twosq * sq(a) * gu1sq * rhosq * (sq(alphaf) + sq(alphas)));
+    const double Term54 = dvz<false>(alphaf, twosq * sq(a) * gu1sq * rhosq * (sq(alphaf) + sq(alphas)));
+    const double Term74 = dvz<false>(alphas, twosq * sq(a) * gu1sq * rhosq * (sq(alphaf) + sq(alphas)));
     // Term51..Term77 of eigenmatrix.f90:287-351 with the zero normal
     // components removed
     double T51, T52, T53, T55, T56, T57, T71, T72, T73, T75, T76, T77;
@@ -715,20 +729,20 @@ GDF_HD void eigenmatrix(const Phys& P, int dir, double rho, double u1, double u2
       T76 = 0.0;
       T77 = -alphaf * t3;
     }
-    lu[4][1] = dv(-T51, nen51);
-    lu[4][2] = dv(T52, nen51);
-    lu[4][3] = dv(T53, nen51);
+    lu[4][1] = dvz<false>(-T51, nen51);
+    lu[4][2] = dvz<false>(T52, nen51);
+    lu[4][3] = dvz<false>(T53, nen51);
     lu[4][4] = Term54;
-    lu[4][5] = dv(T55, nen52);
-    lu[4][6] = dv(T56, nen52);
-    lu[4][7] = dv(T57, nen52);
-    lu[6][1] = dv(T71, nen71);
-    lu[6][2] = dv(T72, nen71);
-    lu[6][3] = dv(T73, nen71);
+    lu[4][5] = dvz<false>(T55, nen52);
+    lu[4][6] = dvz<false>(T56, nen52);
+    lu[4][7] = dvz<false>(T57, nen52);
+    lu[6][1] = dvz<false>(T71, nen71);
+    lu[6][2] = dvz<false>(T72, nen71);
+    lu[6][3] = dvz<false>(T73, nen71);
     lu[6][4] = Term74;
-    lu[6][5] = dv(T75, nen52);
-    lu[6][6] = dv(T76, nen52);
-    lu[6][7] = dv(T77, nen52);
+    lu[6][5] = dvz<false>(T75, nen52);
+    lu[6][6] = dvz<false>(T76, nen52);
+    lu[6][7] = dvz<false>(T77, nen52);
 #pragma unroll
     for (int pr = 2; pr <= 6; pr += 2) {
       lu[pr + 1][0] = lu[pr][0];
@@ -745,10 +759,10 @@ GDF_HD void eigenmatrix(const Phys& P, int dir, double rho, double u1, double u2
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
       const double* l = lu[m];
-      L[m + 8 * 0] = l[0] * g1 - dv(l[1] * u1 * g1, rho) - dv(l[2] * u2 * g1, rho) - dv(l[3] * u3 * g1, rho) + l[4] * g12 * k2 * .5;
-      L[m + 8 * 1] = -l[4] * u1 * g12 + dv(l[1] * g1, rho);
-      L[m + 8 * 2] = -l[4] * u2 * g12 + dv(l[2] * g1, rho);
-      L[m + 8 * 3] = -l[4] * u3 * g12 + dv(l[3] * g1, rho);
+      L[m + 8 * 0] = l[0] * g1 - dvz<false>(l[1] * u1 * g1, rho) - dvz<false>(l[2] * u2 * g1, rho) - dvz<false>(l[3] * u3 * g1, rho) + l[4] * g12 * k2 * .5;
+      L[m + 8 * 1] = -l[4] * u1 * g12 + dvz<false>(l[1] * g1, rho);
+      L[m + 8 * 2] = -l[4] * u2 * g12 + dvz<false>(l[2] * g1, rho);
+      L[m + 8 * 3] = -l[4] * u3 * g12 + dvz<false>(l[3] * g1, rho);
       L[m + 8 * 4] = l[4] * g12;
       L[m + 8 * 5] = l[5] * g1 - B1 * l[4] * g12;
       L[m + 8 * 6] = l[6] * g1 - B2 * l[4] * g12;
