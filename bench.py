@@ -281,7 +281,18 @@ def make_blast(gdf, detector, net=None, lo=0.5, hi=0.5):
     return s, cfg, tend, setup_s
 
 
-def residual_roofline(prof, ncell, hbm_peak, peak_kind, fp64_tflops, counters, step_ms):
+def step_flops(problem: str = "blast"):
+    """Exact FP64 operations per cell-update of a step (the counting build
+    of the oracle, oracle/count_flops.py, saved under profiles/)."""
+    p = os.path.join(REPO, "profiles", "flops_per_cell_update.json")
+    try:
+        with open(p) as f:
+            return json.load(f)[problem]["flop_per_cell_update"]
+    except Exception:
+        return None
+
+
+def residual_roofline(prof, ncell, hbm_peak, peak_kind, fp64_tflops, counters, step_ms, problem="blast"):
     """Roofline of the residual kernel (the stage's main kernel, one launch
     per stage): algorithmic bytes = one stage's share of the step's 2752 B
     per cell; measured time = its event-timed launches."""
@@ -300,6 +311,14 @@ def residual_roofline(prof, ncell, hbm_peak, peak_kind, fp64_tflops, counters, s
            "step": {"alg_bytes_per_cell_update": STEP_BYTES_PER_CELL, "ms": step_ms,
                     "achieved_gbs": STEP_BYTES_PER_CELL * ncell / (step_ms / 1e3) / 1e9,
                     "frac": STEP_BYTES_PER_CELL * ncell / (step_ms / 1e3) / 1e9 / hbm_peak}}
+    fl = step_flops(problem)
+    if fl and fp64_tflops:
+        tf = fl * ncell / (step_ms / 1e3) / 1e12
+        out["step"]["fp64"] = {"alg_flop_per_cell_update": fl, "achieved_tflops": tf, "peak_tflops": fp64_tflops,
+                               "frac": tf / fp64_tflops,
+                               "source": "profiles/flops_per_cell_update.json (oracle/count_flops.py)",
+                               "note": "peak = measured FMA rate (2 flop per FMA); the product build forms no FMA, "
+                                       "so its own ceiling is half of it"}
     if traffic:
         out["traffic_source"] = c.get("source")
     if fp64_tflops:
@@ -346,7 +365,8 @@ def rotor_extra(gdf, steps: int, hbm_peak, peak_kind, fp64_tflops):
         r = {"value": 512 * 512 * k / (ms / 1e3), "ms_per_step": ms / k, "steps": k}
         if exact:
             prof = s.profile(2)
-            r["roofline"] = residual_roofline(prof, 512 * 512, hbm_peak, peak_kind, fp64_tflops, {}, ms / k)
+            r["roofline"] = residual_roofline(prof, 512 * 512, hbm_peak, peak_kind, fp64_tflops, {}, ms / k,
+                                              problem="rotor")
             r["kernels_ms_per_launch"] = {kk: v[0] for kk, v in prof.items() if v[1]}
         s.close()
         out[name] = r
@@ -368,6 +388,27 @@ def learned_blast512(gdf):
                         "gated_cells_per_step": g_l},
             "speedup": ms_p * st_p / (ms_l * st_l),
             "l1_rho_learned_vs_plain": float(np.abs(rho_l - rho_p).mean() / np.abs(rho_p).mean())}
+
+
+def mlp_train_bench(gdf):
+    """Indicator training throughput with the products on tcgen05 (UMMA,
+    tensor-memory accumulators, the default) and on mma.sync, 4 epochs
+    over 262144 synthetic samples, batch 2048, after one warm-up epoch."""
+    import numpy as np
+    rng = np.random.default_rng(0)
+    X = rng.normal(0, 1, (262144, gdf.NFEAT)).astype(np.float32)
+    y = (X[:, :8].sum(1) > 1.0).astype(np.float32)
+    out = {"samples": len(y), "batch": 2048, "epochs": 4}
+    for name, tc in (("tcgen05", True), ("mma_sync", False)):
+        m = gdf.Mlp(0)
+        m.set_products(tc)
+        m.train(X, y, epochs=1, batch=2048, lr=1e-3)
+        t0 = time.perf_counter()
+        loss = m.train(X, y, epochs=4, batch=2048, lr=1e-3)
+        el = time.perf_counter() - t0
+        out[name] = {"seconds": el, "samples_per_s": 4 * len(y) / el, "final_loss": float(loss[-1])}
+        m.close()
+    return out
 
 
 def ensemble_bench(gdf, steps: int):
@@ -599,7 +640,8 @@ def run_ours(args):
     if not args.no_extra and rank == 0 and world == 1:
         for name, fn in (("rotor512_plain", lambda: rotor_extra(gdf, 100, hbm_peak, peak_kind, fp64_tflops)),
                          ("blast512_full_run", lambda: learned_blast512(gdf)),
-                         ("ensemble", lambda: ensemble_bench(gdf, args.steps))):
+                         ("ensemble", lambda: ensemble_bench(gdf, args.steps)),
+                         ("mlp_train", lambda: mlp_train_bench(gdf))):
             try:
                 extras[name] = fn()
             except Exception as e:   # reported, not fatal: the headline line still prints

@@ -18,7 +18,10 @@
 // (no Fortran compiler in the image). The restatement is pinned instead by
 // the invariants the reference's own diagnostics check (conservation,
 // totaldiv at round-off, calculate_L2error convergence on init1.txt) and
-// by hand-derived known answers for the pointwise routines, in tests/.
+// by known answers of the published methods for the pointwise routines
+// (Rusanov, HLL, Toro's HLLC, Li's HLLC-C, Miyoshi-Kusano's HLLD, the
+// ideal-MHD wave speeds of the eigensystem), with the reference's own
+// departures from them written as closed-form terms, in tests/.
 //
 // Build: oracle/Makefile (g++ -O2 -ffp-contract=off, x86-64 baseline ISA,
 // so no FMA is formed, as in a gfortran -O3 build without -march).

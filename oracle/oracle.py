@@ -21,6 +21,7 @@ sys.path.insert(0, os.path.join(REPO, "freljord-cfd-arsenal_b200"))
 from gdf._abi import (GdfConfig, dptr, iptr, new_state)  # noqa: E402
 
 LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+COUNT_LIB_PATH = os.path.join(HERE, "_build", "liboracle_count.so")
 
 
 def build() -> str:
@@ -29,6 +30,35 @@ def build() -> str:
 
 
 _lib = None
+_count_lib = None
+
+
+def _declare(L):
+    vp, dp, ip = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int32)
+    L.orc_create.restype = vp
+    L.orc_create.argtypes = [C.POINTER(GdfConfig)]
+    L.orc_destroy.argtypes = [vp]
+    L.orc_threads.argtypes = [C.c_int]
+    L.orc_threads.restype = C.c_int
+    L.orc_init_data.argtypes = [vp, C.c_int, dp, dp, dp, dp]
+    L.orc_set_bc.argtypes = [vp, dp]
+    L.orc_lh.argtypes = [vp, dp, dp]
+    L.orc_lhez.argtypes = [vp, dp, dp, dp]
+    L.orc_limit.argtypes = [vp, dp, dp, dp, ip]
+    L.orc_div_free.argtypes = [vp, dp, dp, dp]
+    L.orc_dt.argtypes = [vp, dp, dp]
+    L.orc_prepare.argtypes = [vp, dp, dp, dp, ip]
+    L.orc_step.argtypes = [vp, dp, dp, dp, dp, C.c_double, dp, ip]
+    L.orc_diagnostics.argtypes = [vp, dp, dp, dp, dp]
+    L.orc_reset_trouble.argtypes = [vp]
+    L.orc_eigenvalue.argtypes = [vp, dp, C.c_int, C.c_int, dp, dp]
+    L.orc_eigenmatrix.argtypes = [vp, dp, dp, dp, dp]
+    L.orc_riemann.argtypes = [vp, dp, dp, C.c_int, dp]
+    L.orc_vertex_ez.argtypes = [vp, dp, dp, dp, dp]
+    L.orc_vertex_ez.restype = C.c_double
+    L.orc_pow_hxhy.argtypes = [vp]
+    L.orc_pow_hxhy.restype = C.c_double
+    return L
 
 
 def lib():
@@ -36,33 +66,21 @@ def lib():
     if _lib is None:
         if not os.path.exists(LIB_PATH):
             build()
-        L = C.CDLL(LIB_PATH)
-        vp, dp, ip = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int32)
-        L.orc_create.restype = vp
-        L.orc_create.argtypes = [C.POINTER(GdfConfig)]
-        L.orc_destroy.argtypes = [vp]
-        L.orc_threads.argtypes = [C.c_int]
-        L.orc_threads.restype = C.c_int
-        L.orc_init_data.argtypes = [vp, C.c_int, dp, dp, dp, dp]
-        L.orc_set_bc.argtypes = [vp, dp]
-        L.orc_lh.argtypes = [vp, dp, dp]
-        L.orc_lhez.argtypes = [vp, dp, dp, dp]
-        L.orc_limit.argtypes = [vp, dp, dp, dp, ip]
-        L.orc_div_free.argtypes = [vp, dp, dp, dp]
-        L.orc_dt.argtypes = [vp, dp, dp]
-        L.orc_prepare.argtypes = [vp, dp, dp, dp, ip]
-        L.orc_step.argtypes = [vp, dp, dp, dp, dp, C.c_double, dp, ip]
-        L.orc_diagnostics.argtypes = [vp, dp, dp, dp, dp]
-        L.orc_reset_trouble.argtypes = [vp]
-        L.orc_eigenvalue.argtypes = [vp, dp, C.c_int, C.c_int, dp, dp]
-        L.orc_eigenmatrix.argtypes = [vp, dp, dp, dp, dp]
-        L.orc_riemann.argtypes = [vp, dp, dp, C.c_int, dp]
-        L.orc_vertex_ez.argtypes = [vp, dp, dp, dp, dp]
-        L.orc_vertex_ez.restype = C.c_double
-        L.orc_pow_hxhy.argtypes = [vp]
-        L.orc_pow_hxhy.restype = C.c_double
-        _lib = L
+        _lib = _declare(C.CDLL(LIB_PATH))
     return _lib
+
+
+def count_lib():
+    """The oracle built on the counting scalar (flopcount.h): same values,
+    single-threaded, with a tally of its + - * / and square roots."""
+    global _count_lib
+    if _count_lib is None:
+        if not os.path.exists(COUNT_LIB_PATH):
+            build()
+        L = _declare(C.CDLL(COUNT_LIB_PATH))
+        L.orc_flops.argtypes = [C.POINTER(C.c_uint64)]
+        _count_lib = L
+    return _count_lib
 
 
 def set_threads(n: int = 0) -> int:
@@ -72,17 +90,18 @@ def set_threads(n: int = 0) -> int:
 class Oracle:
     """One oracle instance per configuration (holds the sticky KXRCF flags)."""
 
-    def __init__(self, cfg: GdfConfig):
+    def __init__(self, cfg: GdfConfig, counting: bool = False):
         self.cfg = cfg.copy()
         self.nx, self.ny = cfg.nx, cfg.ny
-        self.h = lib().orc_create(C.byref(self.cfg))
+        self.L = count_lib() if counting else lib()
+        self.h = self.L.orc_create(C.byref(self.cfg))
         if not self.h:
             raise ValueError("bad oracle configuration")
 
     def __del__(self):
         h = getattr(self, "h", None)
-        if h and _lib is not None:
-            _lib.orc_destroy(h)
+        if h and getattr(self, "L", None) is not None:
+            self.L.orc_destroy(h)
             self.h = None
 
     def state(self):
@@ -94,77 +113,87 @@ class Oracle:
     def init_data(self, problem: int, params=None):
         uh, bx, by = self.state()
         p = None if params is None else dptr(np.ascontiguousarray(params, np.float64))
-        lib().orc_init_data(self.h, problem, p, dptr(uh), dptr(bx), dptr(by))
+        self.L.orc_init_data(self.h, problem, p, dptr(uh), dptr(bx), dptr(by))
         return uh, bx, by
 
     def set_bc(self, uh):
-        lib().orc_set_bc(self.h, dptr(uh))
+        self.L.orc_set_bc(self.h, dptr(uh))
 
     def lh(self, uh):
         du = np.zeros_like(uh)
-        lib().orc_lh(self.h, dptr(uh), dptr(du))
+        self.L.orc_lh(self.h, dptr(uh), dptr(du))
         return du
 
     def lhez(self, uh):
         _, d1, d2 = self.state()
-        lib().orc_lhez(self.h, dptr(uh), dptr(d1), dptr(d2))
+        self.L.orc_lhez(self.h, dptr(uh), dptr(d1), dptr(d2))
         return d1, d2
 
     def limit(self, uh, bx, by):
         f = self.flags()
-        lib().orc_limit(self.h, dptr(uh), dptr(bx), dptr(by), iptr(f))
+        self.L.orc_limit(self.h, dptr(uh), dptr(bx), dptr(by), iptr(f))
         return f
 
     def div_free(self, uh, bx, by):
-        lib().orc_div_free(self.h, dptr(uh), dptr(bx), dptr(by))
+        self.L.orc_div_free(self.h, dptr(uh), dptr(bx), dptr(by))
 
     def dt(self, uh) -> float:
         d = C.c_double()
-        lib().orc_dt(self.h, dptr(uh), C.byref(d))
+        self.L.orc_dt(self.h, dptr(uh), C.byref(d))
         return d.value
 
     def prepare(self, uh, bx, by):
         f = self.flags()
-        lib().orc_prepare(self.h, dptr(uh), dptr(bx), dptr(by), iptr(f))
+        self.L.orc_prepare(self.h, dptr(uh), dptr(bx), dptr(by), iptr(f))
         return f
 
     def step(self, uh, bx, by, t: float, tend: float):
         tt = C.c_double(t)
         dt = C.c_double()
         f = self.flags()
-        lib().orc_step(self.h, dptr(uh), dptr(bx), dptr(by), C.byref(tt), tend, C.byref(dt), iptr(f))
+        self.L.orc_step(self.h, dptr(uh), dptr(bx), dptr(by), C.byref(tt), tend, C.byref(dt), iptr(f))
         return tt.value, dt.value, f
 
     def diagnostics(self, uh):
         a, b, c = C.c_double(), C.c_double(), C.c_double()
-        lib().orc_diagnostics(self.h, dptr(uh), C.byref(a), C.byref(b), C.byref(c))
+        self.L.orc_diagnostics(self.h, dptr(uh), C.byref(a), C.byref(b), C.byref(c))
         return a.value, b.value, c.value
 
     def reset_trouble(self):
-        lib().orc_reset_trouble(self.h)
+        self.L.orc_reset_trouble(self.h)
 
     # pointwise known-answer entry points
     def eigenvalue(self, U8, n1: int, n2: int):
         a, b = C.c_double(), C.c_double()
-        lib().orc_eigenvalue(self.h, dptr(np.ascontiguousarray(U8, np.float64)), n1, n2, C.byref(a), C.byref(b))
+        self.L.orc_eigenvalue(self.h, dptr(np.ascontiguousarray(U8, np.float64)), n1, n2, C.byref(a), C.byref(b))
         return a.value, b.value
 
     def eigenmatrix(self, prim8, n3):
         R = np.zeros(64)
         L = np.zeros(64)
-        lib().orc_eigenmatrix(self.h, dptr(np.ascontiguousarray(prim8, np.float64)),
+        self.L.orc_eigenmatrix(self.h, dptr(np.ascontiguousarray(prim8, np.float64)),
                               dptr(np.ascontiguousarray(n3, np.float64)), dptr(R), dptr(L))
         return R.reshape(8, 8).T.copy(), L.reshape(8, 8).T.copy()   # row-major R[r, c]
 
     def riemann(self, ul, ur, direction: int):
         f = np.zeros(8)
-        lib().orc_riemann(self.h, dptr(np.ascontiguousarray(ul, np.float64)),
+        self.L.orc_riemann(self.h, dptr(np.ascontiguousarray(ul, np.float64)),
                           dptr(np.ascontiguousarray(ur, np.float64)), direction, dptr(f))
         return f
 
     def vertex_ez(self, uru, ulu, urd, uld) -> float:
         a = [dptr(np.ascontiguousarray(v, np.float64)) for v in (uru, ulu, urd, uld)]
-        return lib().orc_vertex_ez(self.h, *a)
+        return self.L.orc_vertex_ez(self.h, *a)
 
     def pow_hxhy(self) -> float:
-        return lib().orc_pow_hxhy(self.h)
+        return self.L.orc_pow_hxhy(self.h)
+
+    # flop tally of the counting build: (add, mul, div, sqrt, pow) since the
+    # last reset
+    def flops(self):
+        f = (C.c_uint64 * 5)()
+        self.L.orc_flops(f)
+        return tuple(int(v) for v in f)
+
+    def reset_flops(self):
+        self.L.orc_flops_reset()
