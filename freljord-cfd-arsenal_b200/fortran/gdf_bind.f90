@@ -55,6 +55,14 @@ module gdf_bind
       type(c_ptr), value :: h
       real(c_double), intent(out) :: uh(*), bx(*), by(*)
     end function
+    ! init_data.f90 on the device, into the handle's state (params may be
+    ! c_null_ptr for the problem's defaults)
+    integer(c_int) function gdf_init_data_device(h, problem, params) bind(c, name="gdf_init_data_device")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int), value :: problem
+      type(c_ptr), value :: params
+    end function
     integer(c_int) function gdf_prepare(h, flags) bind(c, name="gdf_prepare")
       import :: c_int, c_ptr
       type(c_ptr), value :: h
