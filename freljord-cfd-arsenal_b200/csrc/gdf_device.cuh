@@ -73,6 +73,12 @@ __device__ __forceinline__ void set_bc_item(const Consts& K, double* __restrict_
   U[off + i + (long long)K.nx2 * j] = v;
 }
 
+// Products with the exact 1 and -1 entries of the basis tables written as
+// the value itself (x * 1 == x, x * -1 == -x for every double)
+#ifndef GDF_FOLD_UNIT
+#define GDF_FOLD_UNIT 1
+#endif
+
 // ---------------------------------------------------- face Riemann -------
 // Lh.f90:72-265 and LhEz.f90:6-31 for one face quadrature point.
 // DIR 0: x face (i = 0..Nx, j = 1..Ny) between cells (i,j) and (i+1,j).
@@ -97,8 +103,20 @@ __device__ __forceinline__ void face_point(const Consts& K, ML mL, MR mR, int g,
       if (!live_mode(n, d)) continue;
       const double pl = DIR == 0 ? c_basis.phiGR[g][d] : c_basis.phiGU[g][d];
       const double pr = DIR == 0 ? c_basis.phiGL[g][d] : c_basis.phiGD[g][d];
-      a = a + mL(n, d) * pl;
-      b = b + mR(n, d) * pr;
+      // the face basis is 1 for mode 1, and for mode 2 (x faces) or 3 (y
+      // faces) 1 on the low cell's face and -1 on the high cell's
+      // (get_basis.f90): those products are exact and written out
+      const int du = DIR == 0 ? 1 : 2;
+      if (GDF_FOLD_UNIT && d == 0) {
+        a = a + mL(n, d);
+        b = b + mR(n, d);
+      } else if (GDF_FOLD_UNIT && d == du) {
+        a = a + mL(n, d);
+        b = b + (-mR(n, d));
+      } else {
+        a = a + mL(n, d) * pl;
+        b = b + mR(n, d) * pr;
+      }
     }
     uL[n] = a;
     uR[n] = b;
@@ -250,8 +268,12 @@ __device__ __forceinline__ void cell_item(const Consts& K, const double* __restr
         for (int n = 0; n < NE; ++n) {
           double acc = 0.0;
 #pragma unroll
-          for (int d = 0; d < NP; ++d)
-            if (live_mode(n, d)) acc = acc + ms[LI(n, d) * CELL_BS + tid] * c_basis.phiG[a][b][d];
+          for (int d = 0; d < NP; ++d) {
+            if (!live_mode(n, d)) continue;
+            // mode 1 of the volume basis is 1 at every point: m * 1 == m
+            if (GDF_FOLD_UNIT && d == 0) acc = acc + ms[LI(n, d) * CELL_BS + tid];
+            else acc = acc + ms[LI(n, d) * CELL_BS + tid] * c_basis.phiG[a][b][d];
+          }
           v[n] = acc;
         }
         const double rho = v[0];
@@ -321,12 +343,23 @@ __device__ __forceinline__ void cell_item(const Consts& K, const double* __restr
 #pragma unroll
         for (int g = 0; g < NG; ++g) {
           if (g == 2 && (d == 2 || d == 4 || d == 7 || d == 9)) continue;
-          acc = acc - K.cxs * c_basis.w[g] * (fr[g] * c_basis.phiGR[g][d] - fl[g] * c_basis.phiGL[g][d]);
+          // modes 1 and 2 of the x-face basis are 1 on the right face and
+          // +-1 on the left (get_basis.f90): x * 1 and x * -1 are exact, so
+          // those products are written out
+          const double t = (GDF_FOLD_UNIT && d == 0) ? fr[g] - fl[g]
+                           : (GDF_FOLD_UNIT && d == 1) ? fr[g] - (-fl[g])
+                                                       : fr[g] * c_basis.phiGR[g][d] - fl[g] * c_basis.phiGL[g][d];
+          acc = acc - K.cxs * c_basis.w[g] * t;
         }
 #pragma unroll
         for (int g = 0; g < NG; ++g) {
           if (g == 2 && (d == 1 || d == 4 || d == 8 || d == 6)) continue;
-          acc = acc - K.cys * c_basis.w[g] * (fu[g] * c_basis.phiGU[g][d] - fd[g] * c_basis.phiGD[g][d]);
+          // modes 1 and 3 of the y-face basis: 1 on the upper face, +-1 on
+          // the lower
+          const double t = (GDF_FOLD_UNIT && d == 0) ? fu[g] - fd[g]
+                           : (GDF_FOLD_UNIT && d == 2) ? fu[g] - (-fd[g])
+                                                       : fu[g] * c_basis.phiGU[g][d] - fd[g] * c_basis.phiGD[g][d];
+          acc = acc - K.cys * c_basis.w[g] * t;
         }
         du[LI(n, d)] = (n == 3 || n == 7) ? dv(acc, c_basis.mm[d]) : acc / c_basis.mm[d];
       }

@@ -28,6 +28,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/gdf.h"
@@ -677,21 +678,49 @@ static size_t uh_bytes(const GdfConfig& c) { return (size_t)(c.nx + 2) * (c.ny +
 static size_t bx_bytes(const GdfConfig& c) { return (size_t)(c.nx + 1) * c.ny * 3 * sizeof(double); }
 static size_t by_bytes(const GdfConfig& c) { return (size_t)c.nx * (c.ny + 1) * 3 * sizeof(double); }
 
-// dead (mode, variable) slots must be zero in an uploaded state
+// dead (mode, variable) slots must be zero in an uploaded state. The 28
+// dead planes are scanned by several host threads (a 2048^2 state has 940 MB
+// of them; one thread took longer than the upload it overlaps); the error
+// names the first failing slot in (variable, mode) order.
 static int check_dead_slots(const GdfConfig& c, const double* uh) {
   const size_t plane = (size_t)(c.nx + 2) * (c.ny + 2);
+  std::vector<int> dead;
   for (int n = 0; n < NE; ++n)
-    for (int d = 0; d < NP; ++d) {
-      if (live_mode(n, d)) continue;
-      // +0 and -0 pass, anything else (NaN included) fails: OR of the bit
-      // patterns without the sign bit, a loop the compiler vectorises
-      const uint64_t* w = reinterpret_cast<const uint64_t*>(uh + plane * (d + 10 * n));
-      uint64_t acc = 0;
-      for (size_t q = 0; q < plane; ++q) acc |= w[q] << 1;
-      if (acc != 0)
-        return fail(GDF_ERR_ARG, "uh has a nonzero value in mode " + std::to_string(d + 1) + " of variable " +
-                                     std::to_string(n + 1) + ", which the P2 scheme never populates");
+    for (int d = 0; d < NP; ++d)
+      if (!live_mode(n, d)) dead.push_back(d + 10 * n);
+  // +0 and -0 pass, anything else (NaN included) fails: OR of the bit
+  // patterns without the sign bit, a loop the compiler vectorises
+  auto bad_range = [&](int slot, size_t q0, size_t q1) {
+    const uint64_t* w = reinterpret_cast<const uint64_t*>(uh + plane * slot);
+    uint64_t acc = 0;
+    for (size_t q = q0; q < q1; ++q) acc |= w[q] << 1;
+    return acc != 0;
+  };
+  const size_t total = plane * dead.size();
+  unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  if (total < ((size_t)1 << 22)) nt = 1;
+  std::vector<char> bad(dead.size(), 0);
+  auto work = [&](unsigned t) {
+    // thread t scans a contiguous share of the concatenated dead planes
+    const size_t a = total * t / nt, b = total * (t + 1) / nt;
+    for (size_t k = a; k < b;) {
+      const size_t s = k / plane, q0 = k - s * plane;
+      const size_t q1 = std::min(plane, q0 + (b - k));
+      if (bad_range(dead[s], q0, q1)) bad[s] = 1;
+      k += q1 - q0;
     }
+  };
+  if (nt == 1) {
+    work(0);
+  } else {
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < nt; ++t) th.emplace_back(work, t);
+    for (auto& x : th) x.join();
+  }
+  for (size_t s = 0; s < dead.size(); ++s)
+    if (bad[s])
+      return fail(GDF_ERR_ARG, "uh has a nonzero value in mode " + std::to_string(dead[s] % 10 + 1) + " of variable " +
+                                   std::to_string(dead[s] / 10 + 1) + ", which the P2 scheme never populates");
   return GDF_OK;
 }
 
