@@ -224,10 +224,21 @@ __device__ __forceinline__ void vertex_item(const Consts& K, const double* __res
     for (int d = 0; d < NP; ++d) {
       if (!live_mode(n, d)) continue;
       const long long off = K.plane * (d + 10 * n);
-      a = a + U[off + cRU] * c_basis.phiLD[d];
-      b = b + U[off + cLU] * c_basis.phiRD[d];
-      c = c + U[off + cRD] * c_basis.phiLU[d];
-      e = e + U[off + cLD] * c_basis.phiRU[d];
+      if (GDF_FOLD_UNIT && (d == 0 || d == 1 || d == 2 || d == 4)) {
+        // corner values of modes 1, 2, 3 and 5 are +-1 (get_basis.f90):
+        // phiLD = (1,-1,-1,.,1), phiRD = (1,1,-1,.,-1), phiLU = (1,-1,1,.,-1),
+        // phiRU = (1,1,1,.,1); the products are exact and written out
+        const double xa = U[off + cRU], xb = U[off + cLU], xc = U[off + cRD], xe = U[off + cLD];
+        a = a + ((d == 1 || d == 2) ? -xa : xa);
+        b = b + ((d == 2 || d == 4) ? -xb : xb);
+        c = c + ((d == 1 || d == 4) ? -xc : xc);
+        e = e + xe;
+      } else {
+        a = a + U[off + cRU] * c_basis.phiLD[d];
+        b = b + U[off + cLU] * c_basis.phiRD[d];
+        c = c + U[off + cRD] * c_basis.phiLU[d];
+        e = e + U[off + cLD] * c_basis.phiRU[d];
+      }
     }
     URU[n] = a; ULU[n] = b; URD[n] = c; ULD[n] = e;
   }
@@ -361,7 +372,10 @@ __device__ __forceinline__ void cell_item(const Consts& K, const double* __restr
                                                        : fu[g] * c_basis.phiGU[g][d] - fd[g] * c_basis.phiGD[g][d];
           acc = acc - K.cys * c_basis.w[g] * t;
         }
-        du[LI(n, d)] = (n == 3 || n == 7) ? dv(acc, c_basis.mm[d]) : acc / c_basis.mm[d];
+        // mm(1) = 1 (get_basis.f90): x / 1 == x
+        du[LI(n, d)] = (GDF_FOLD_UNIT && d == 0) ? acc
+                       : (n == 3 || n == 7)     ? dv(acc, c_basis.mm[d])
+                                                : acc / c_basis.mm[d];
       }
     }
   }
