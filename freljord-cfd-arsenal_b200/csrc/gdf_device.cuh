@@ -73,6 +73,11 @@ __device__ __forceinline__ void set_bc_item(const Consts& K, double* __restrict_
   U[off + i + (long long)K.nx2 * j] = v;
 }
 
+// k_cell asks for its faces' fluxes in L2 before its volume loop
+#ifndef GDF_CELL_PREFETCH
+#define GDF_CELL_PREFETCH 1
+#endif
+
 // Products with the exact 1 and -1 entries of the basis tables written as
 // the value itself (x * 1 == x, x * -1 == -x for every double)
 #ifndef GDF_FOLD_UNIT
@@ -269,6 +274,19 @@ __device__ __forceinline__ void cell_item(const Consts& K, const double* __restr
 #pragma unroll
       for (int d = 0; d < NP; ++d)
         if (live_mode(n, d)) ms[LI(n, d) * CELL_BS + tid] = U[item + K.plane * (d + 10 * n)];
+    if (GDF_CELL_PREFETCH) {
+      // the surface term reads the fluxes of the cell's four faces after the
+      // volume loop: ask for them in L2 now, so the loads that follow the
+      // volume work do not wait on DRAM
+      const long long px = (i - 1) + 1 + (long long)(K.nx + 1) * (j - 1);
+      const long long py = (i - 1) + (long long)K.nx * j;
+#pragma unroll 1
+      for (int q = 0; q < NE * NG; ++q) {
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(Fxh + q * K.fxplane + px - 1));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(Fyh + q * K.fyplane + py));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(Fyh + q * K.fyplane + py - K.nx));
+      }
+    }
     // volume term
 #pragma unroll 1
     for (int a = 0; a < NG; ++a) {

@@ -51,6 +51,9 @@
 #ifndef GDF_FACE_STAGED
 #define GDF_FACE_STAGED 0
 #endif
+#ifndef GDF_VERTEX_MINB
+#define GDF_VERTEX_MINB GDF_FACE_MINB
+#endif
 #ifndef GDF_CELL_MINB
 #define GDF_CELL_MINB 1
 #endif
@@ -93,7 +96,7 @@ __global__ void __launch_bounds__(128, GDF_FACE_MINB) k_face_tile(const __grid_c
   face_tile<DIR>(K, U, Fh_out, Ez_out, (int)blockIdx.x * FACE_TILE, (int)blockIdx.y, ms);
 }
 
-__global__ void __launch_bounds__(128, GDF_FACE_MINB) k_vertex(const __grid_constant__ Consts K, const double* __restrict__ U,
+__global__ void __launch_bounds__(128, GDF_VERTEX_MINB) k_vertex(const __grid_constant__ Consts K, const double* __restrict__ U,
                                                 double* __restrict__ EzV, const Scal* __restrict__ sc) {
   if (sc && !sc->active) return;
   const long long item = gtid();
