@@ -51,14 +51,22 @@
 #ifndef GDF_FACE_STAGED
 #define GDF_FACE_STAGED 0
 #endif
+// vertex kernel at 3 blocks (168 registers, no spill): timed alone a
+// launch is 10% slower than at 4 blocks, but the blast 2048^2 step replayed
+// from its graph is 2% shorter (45.9 against 46.9 ms, same values)
 #ifndef GDF_VERTEX_MINB
-#define GDF_VERTEX_MINB GDF_FACE_MINB
+#define GDF_VERTEX_MINB 3
 #endif
 #ifndef GDF_CELL_MINB
 #define GDF_CELL_MINB 1
 #endif
 #ifndef GDF_LIMIT_MINB
 #define GDF_LIMIT_MINB 1
+#endif
+// the learned indicator's stage-1 inference in its own kernel (k_infer)
+// ahead of the limiter, instead of inside the 255-register limiter blocks
+#ifndef GDF_INFER_APART
+#define GDF_INFER_APART 1
 #endif
 
 
@@ -142,6 +150,70 @@ __global__ void k_features(const __grid_constant__ Consts K, const float* __rest
   gather_features(K, QM, i + (long long)K.nx2 * j, f);
 #pragma unroll
   for (int k = 0; k < NFEAT; ++k) X[item * NFEAT + k] = f[k];
+}
+
+// The learned indicator of every interior cell ahead of the stage-1 limiter:
+// resident blocks stage the BF16 weights once and walk the LIM_BS-cell
+// tiles of the grid (features gathered from QM, the two tensor-core
+// products, the sigmoid), storing each cell's probability in pnet. A tile
+// computes what the limiter block with inference computes for the same
+// cells (same features, roundings and product order per row), so the
+// stored probabilities are those of k_limit<LIM_INFER>, at the occupancy of
+// a 128-register kernel instead of the FP64 limiter's 255 registers.
+__global__ void __launch_bounds__(LIM_BS) k_infer(const __grid_constant__ Consts K, const MlpDev* __restrict__ net,
+                                                     const float* __restrict__ QM, float* __restrict__ pnet,
+                                                     const Scal* __restrict__ gate_sc) {
+  extern __shared__ __align__(16) unsigned char lsm[];
+  if (gate_sc && !gate_sc->active) return;
+  __nv_bfloat16* Xs = reinterpret_cast<__nv_bfloat16*>(lsm);
+  __nv_bfloat16* W1t = Xs + LIM_BS * MLP_LDX;
+  __nv_bfloat16* W2t = W1t + MLP_H * MLP_LDX;
+  __nv_bfloat16* H1 = W2t + MLP_H * MLP_LDH;
+  float* zz = reinterpret_cast<float*>(H1 + LIM_BS * MLP_LDH);
+  const int tid = threadIdx.x;
+  const uint4* g1 = reinterpret_cast<const uint4*>(net->W1t);
+  const uint4* g2 = reinterpret_cast<const uint4*>(net->W2t);
+  for (int k = tid; k < MLP_H * (MLP_INP / 8); k += LIM_BS) {
+    const int r = k / (MLP_INP / 8), q = k % (MLP_INP / 8);
+    *reinterpret_cast<uint4*>(W1t + r * MLP_LDX + 8 * q) = g1[k];
+  }
+  for (int k = tid; k < MLP_H * (MLP_H / 8); k += LIM_BS) {
+    const int r = k / (MLP_H / 8), q = k % (MLP_H / 8);
+    *reinterpret_cast<uint4*>(W2t + r * MLP_LDH + 8 * q) = g2[k];
+  }
+  const long long ncell = (long long)K.nx * K.ny;
+  for (long long base = (long long)blockIdx.x * LIM_BS; base < ncell; base += (long long)gridDim.x * LIM_BS) {
+    const long long item = base + tid;
+    const bool valid = item < ncell;
+    float f[MLP_INP];
+    if (valid) {
+      const int i = (int)(item % K.nx) + 1, j = (int)(item / K.nx) + 1;
+      gather_features(K, QM, i + (long long)K.nx2 * j, f);
+    } else {
+#pragma unroll
+      for (int k = 0; k < NFEAT; ++k) f[k] = 0.f;
+    }
+#pragma unroll
+    for (int k = NFEAT; k < MLP_INP; ++k) f[k] = 0.f;
+#pragma unroll
+    for (int q = 0; q < MLP_INP / 8; ++q) {
+      __nv_bfloat162 a = __floats2bfloat162_rn(f[8 * q], f[8 * q + 1]);
+      __nv_bfloat162 b = __floats2bfloat162_rn(f[8 * q + 2], f[8 * q + 3]);
+      __nv_bfloat162 cc = __floats2bfloat162_rn(f[8 * q + 4], f[8 * q + 5]);
+      __nv_bfloat162 d = __floats2bfloat162_rn(f[8 * q + 6], f[8 * q + 7]);
+      uint4 v;
+      v.x = *reinterpret_cast<uint32_t*>(&a);
+      v.y = *reinterpret_cast<uint32_t*>(&b);
+      v.z = *reinterpret_cast<uint32_t*>(&cc);
+      v.w = *reinterpret_cast<uint32_t*>(&d);
+      *reinterpret_cast<uint4*>(Xs + tid * MLP_LDX + 8 * q) = v;
+    }
+    // the weights (first tile) and this tile's rows are in place
+    __syncthreads();
+    // ends with a barrier: zz holds the tile's logits, Xs and H1 are free
+    mlp_infer_tiles(Xs, W1t, W2t, net->b1, net->b2, net->w3, net->b3, H1, zz, LIM_BS);
+    if (valid) pnet[item] = 1.f / (1.f + expf(-zz[tid]));
+  }
 }
 
 template <int LM, bool COMPACT>
@@ -355,6 +427,7 @@ struct GdfHandle {
   int64_t launches = 0;
   int64_t step_launches = 0;
   int dt_blocks = 0;
+  int sms = 0;  // SMs of the handle's device (grid of the resident inference blocks)
   cudaGraphExec_t graph = nullptr;
   // per-kernel timing (gdf_profile): events around every launch when set
   int prof = 0;
@@ -588,6 +661,20 @@ static int launch_limit(GdfHandle* h, const double* S, double* D, int stage, con
     if (!h->net || !h->QM) return fail(GDF_ERR_STATE, "detector GDF_DETECT_LEARNED needs gdf_set_indicator first");
     if (infer) {
       int rq = run_kernel(h, GDF_K_LIMIT, [&] { k_qmodes<<<nblk(K.plane, 128), 128, 0, h->st>>>(K, S, h->QM); });
+      if (!rq && GDF_INFER_APART) {
+        const long long tiles = (long long)nblk(ncell, LIM_BS);
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_infer, LIM_BS, LIMIT_SMEM_LEARNED) !=
+                cudaSuccess ||
+            per_sm <= 0) {
+          cudaGetLastError();
+          per_sm = 1;
+        }
+        const unsigned nb = (unsigned)std::min<long long>(tiles, (long long)per_sm * h->sms);
+        rq = run_kernel(h, GDF_K_LIMIT, [&] {
+          k_infer<<<nb, LIM_BS, LIMIT_SMEM_LEARNED, h->st>>>(K, h->net, h->QM, h->pnet, sc_gate);
+        });
+      }
       if (rq) return rq;
       smem = LIMIT_SMEM_LEARNED;
     }
@@ -602,7 +689,7 @@ static int launch_limit(GdfHandle* h, const double* S, double* D, int stage, con
   int32_t *L = h->lim_list, *N = h->lim_count;
   int rc0 = run_kernel(h, GDF_K_LIMIT, [&] {
     const unsigned nb = nblk(ncell, LIM_BS);
-    if (K.detector == GDF_DETECT_LEARNED && infer)
+    if (K.detector == GDF_DETECT_LEARNED && infer && !GDF_INFER_APART)
       k_limit<LIM_INFER, false><<<nb, LIM_BS, smem, h->st>>>(K, S, D, h->BX, h->BY, h->flags, h->trouble, stage,
                                                              fused_divfree, sc_gate, h->sc, h->net, h->QM, h->pnet,
                                                              h->t_lo, h->t_hi, nullptr, nullptr);
@@ -820,6 +907,15 @@ int gdf_create(const GdfConfig* cfg, GdfHandle** out) {
   const size_t fyb = (size_t)h->K.fyplane * NG * NE * sizeof(double);
   const long long ncell = (long long)c.nx * c.ny;
   h->dt_blocks = (int)nblk(ncell, DT_BS);
+  {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || h->sms <= 0) {
+      cudaGetLastError();
+      delete h;
+      return fail(GDF_ERR_CUDA, "querying the device's SM count failed");
+    }
+  }
   auto alloc = [&](void** p, size_t bytes) -> bool {
     if (cudaMalloc(p, bytes) != cudaSuccess) return false;
     return cudaMemset(*p, 0, bytes) == cudaSuccess;
