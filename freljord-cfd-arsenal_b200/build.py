@@ -31,11 +31,12 @@ ENS_SRC = os.path.join(CSRC, "gdf_ensemble.cu")
 PEAK_SRC = os.path.join(CSRC, "gdf_peak.cu")
 INIT_SRC = os.path.join(CSRC, "gdf_init.cu")
 MLPTC_SRC = os.path.join(CSRC, "gdf_mlp_tc.cu")
+P3_SRC = os.path.join(CSRC, "gdf_p3.cu")
 HOST_SRC = os.path.join(CSRC, "gdf_host.cpp")
 IO_SRC = os.path.join(CSRC, "gdf_io.cpp")
 HEADERS = [os.path.join(CSRC, f) for f in ("gdf_physics.cuh", "gdf_kernels.cuh", "gdf_device.cuh",
-                                                         "gdf_mlp.cuh")] + [
-    os.path.join(REPO, "include", "gdf.h")]
+                                                         "gdf_mlp.cuh", "gdf_p3_basis.h")] + [
+    os.path.join(REPO, "include", "gdf.h"), os.path.join(REPO, "include", "gdf_p3.h")]
 
 
 def _nvcc() -> str:
@@ -77,7 +78,7 @@ def build(verbose: bool = False, jobs: int | None = None) -> dict:
     for name, flags in (("libgdf_b200.so", ["--fmad=false", "-DGDF_EXACT=1"]),
                         ("libgdf_b200_fma.so", ["--fmad=true"])):
         objs = []
-        for src in (KERNEL_SRC, MLP_SRC, ENS_SRC, PEAK_SRC, INIT_SRC, MLPTC_SRC):
+        for src in (KERNEL_SRC, MLP_SRC, ENS_SRC, PEAK_SRC, INIT_SRC, MLPTC_SRC, P3_SRC):
             obj = os.path.join(BUILD, name.replace(".so", "") + "_" + os.path.basename(src).replace(".cu", ".o"))
             if _stale(obj, [src] + HEADERS):
                 cmd = [nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17", *flags,

@@ -8,6 +8,8 @@
 #include <vector>
 
 #include "../../include/gdf.h"
+#include "../../include/gdf_p3.h"
+#include "gdf_p3_basis.h"
 
 namespace {
 
@@ -376,6 +378,214 @@ int gdf_l2_error(const GdfConfig* cfg, const double* uh, double t20, double* L2)
         }
     }
   for (int n = 0; n < NE; ++n) L2[n] = std::sqrt(acc[n] * hx1 * hy1);
+  return GDF_OK;
+}
+
+}  // extern "C"
+
+// ======================================================== the k = 3 variant ==
+// MPI_BalsaraP3/main.f90 on one rank: basis tables, presets, initial data.
+
+namespace gdf3 {
+
+// get_basis (main.f90:782-1119). Every product and quotient is written as
+// the Fortran expression evaluates it (x**2 = x*x, x**3 = (x*x)*x,
+// x**4 = (x*x)*(x*x)), so the tables equal a build of the reference.
+void build_basis_p3(double hx1, double hy1, BasisP3* b) {
+  std::memset(b, 0, sizeof(*b));
+  for (int g = 0; g < NG; ++g) {
+    b->lambda[g] = kLam[g];
+    b->weight[g] = kW[g];
+  }
+  const double t3 = 1.0 / 3.0, t23 = 2.0 / 3.0, t25 = 2.0 / 5.0, t35 = 3.0 / 5.0, t835 = 8.0 / 35.0;
+  // the 1-D Legendre polynomials P2..P4 as get_basis writes them
+  auto L2 = [&](double x) { return x * x - t3; };
+  auto L3 = [&](double x) { return x * x * x - 3.0 * x / 5.0; };
+  auto L4 = [&](double x) { return (x * x) * (x * x) - 6 * (x * x) / 7.0 + 3.0 / 35.0; };
+  auto D3 = [&](double x) { return 3 * (x * x) - t35; };                  // 3*x**2 - 3/5
+  auto D4 = [&](double x) { return 4 * (x * x * x) - 12 * x / 7.0; };     // 4*x**3 - 12*x/7
+  for (int a = 0; a < NG; ++a)
+    for (int c = 0; c < NG; ++c) {
+      const double x = kLam[a], y = kLam[c];
+      const double G[NP3] = {1, x, y, L2(x), x * y, L2(y), L3(x), L2(x) * y, x * L2(y), L3(y), L4(x), L3(x) * y,
+                             L2(x) * L2(y), x * L3(y), L4(y)};
+      const double X[NP3] = {0, 1.0 / hx1, 0, 2.0 * x / hx1, y / hx1, 0, D3(x) / hx1, 2.0 * x * y / hx1,
+                             L2(y) / hx1, 0, D4(x) / hx1, D3(x) * y / hx1, 2 * x * L2(y) / hx1, L3(y) / hx1, 0};
+      const double Y[NP3] = {0, 0, 1.0 / hy1, 0, x / hy1, 2.0 * y / hy1, 0, L2(x) / hy1, 2.0 * x * y / hy1,
+                             D3(y) / hy1, 0, L3(x) / hy1, L2(x) * 2 * y / hy1, x * D3(y) / hy1, D4(y) / hy1};
+      for (int d = 0; d < NP3; ++d) {
+        b->phiG[a][c][d] = G[d];
+        b->phixG[a][c][d] = X[d];
+        b->phiyG[a][c][d] = Y[d];
+      }
+    }
+  for (int g = 0; g < NG; ++g) {
+    const double l = kLam[g];
+    const double R[NP3] = {1, 1, l, t23, l, L2(l), t25, t23 * l, L2(l), L3(l), t835, t25 * l, t23 * L2(l), L3(l), L4(l)};
+    const double Lf[NP3] = {1, -1, l, t23, -l, L2(l), -t25, t23 * l, -L2(l), L3(l), t835, -(t25 * l), t23 * L2(l),
+                            -L3(l), L4(l)};
+    const double Uf[NP3] = {1, l, 1, L2(l), l, t23, L3(l), L2(l), l * t23, t25, L4(l), L3(l), L2(l) * t23, l * t25,
+                            t835};
+    const double Df[NP3] = {1, l, -1, L2(l), -l, t23, L3(l), -L2(l), l * t23, -t25, L4(l), -L3(l), L2(l) * t23,
+                            -(l * t25), t835};
+    for (int d = 0; d < NP3; ++d) {
+      b->phiGR[g][d] = R[d];
+      b->phiGL[g][d] = Lf[d];
+      b->phiGU[g][d] = Uf[d];
+      b->phiGD[g][d] = Df[d];
+    }
+    const double E[NB3] = {1, l, L2(l), l * l * l - t35 * l};
+    const double Ex[NB3] = {0, 1 / hx1, 2 * l / hx1, D3(l) / hx1};
+    const double Ey[NB3] = {0, 1 / hy1, 2 * l / hy1, D3(l) / hy1};
+    for (int d = 0; d < NB3; ++d) {
+      b->EzG[g][d] = E[d];
+      b->EzxG[g][d] = Ex[d];
+      b->EzyG[g][d] = Ey[d];
+    }
+  }
+  const double t49 = 4.0 / 9.0;
+  const double RU[NP3] = {1, 1, 1, t23, 1, t23, t25, t23, t23, t25, t835, t25, t49, t25, t835};
+  const double LU[NP3] = {1, -1, 1, t23, -1, t23, -t25, t23, -t23, t25, t835, -t25, t49, -t25, t835};
+  const double RD[NP3] = {1, 1, -1, t23, -1, t23, t25, -t23, t23, -t25, t835, -t25, t49, -t25, t835};
+  const double LD[NP3] = {1, -1, -1, t23, 1, t23, -t25, -t23, -t23, -t25, t835, t25, t49, t25, t835};
+  const double MM[NP3] = {1, 1.0 / 3.0, 1.0 / 3.0, 4.0 / 45.0, 1.0 / 9.0, 4.0 / 45.0, 4.0 / 175.0, 4.0 / 135.0,
+                          4.0 / 135.0, 4.0 / 175.0, 64.0 / 11025.0, 4.0 / 525.0, 16.0 / 2025.0, 4.0 / 525.0,
+                          64.0 / 11025.0};
+  for (int d = 0; d < NP3; ++d) {
+    b->phiRU[d] = RU[d];
+    b->phiLU[d] = LU[d];
+    b->phiRD[d] = RD[d];
+    b->phiLD[d] = LD[d];
+    b->mm[d] = MM[d];
+  }
+  const double ER[NB3] = {1, 1, t23, t25}, EL[NB3] = {1, -1, t23, -t25};
+  const double ME[NB3] = {1, 1.0 / 3.0, 4.0 / 45.0, 4.0 / 175.0};
+  for (int d = 0; d < NB3; ++d) {
+    b->EzR[d] = ER[d];
+    b->EzL[d] = EL[d];
+    b->mmE[d] = ME[d];
+  }
+}
+
+}  // namespace gdf3
+
+extern "C" {
+
+// mesh subroutines of the init modules (main.f90:126-155 init1, 197-226
+// init3, 310-339 init4, 458-489 init6) and the module constants
+int gdf_p3_config_problem(int32_t problem, int32_t nx, int32_t ny, GdfP3Config* cfg, double* tend) {
+  if (!cfg || nx < 2 || ny < 2) return GDF_ERR_ARG;
+  std::memset(cfg, 0, sizeof(*cfg));
+  cfg->nx = nx;
+  cfg->ny = ny;
+  cfg->flux_type = GDF_FLUX_HLL;   // main.f90:9
+  cfg->gamma = 5.0 / 3.0;          // main.f90:19
+  cfg->cfl = 0.75;                 // main.f90:1319
+  cfg->hlld_eps = 1e-6;            // main.f90:2495
+  cfg->change_tol = 1e-13;         // main.f90:3330
+  cfg->tvb_beta = 1;
+  const double pi = 4 * std::atan(1.0);
+  int bc = GDF_BC_PERIODIC;
+  double te = 0;
+  switch (problem) {
+    case GDF_PROB_VORTEX:
+      cfg->xa = -10; cfg->xb = 10; cfg->ya = -10; cfg->yb = 10;
+      te = 20; cfg->tvb_m = 100000000;
+      break;
+    case GDF_PROB_ORSZAG_TANG:
+      cfg->xa = 0; cfg->xb = 2 * pi; cfg->ya = 0; cfg->yb = 2 * pi;
+      te = 3; cfg->tvb_m = 10;
+      break;
+    case GDF_PROB_ROTOR:
+      cfg->xa = 0; cfg->xb = 1; cfg->ya = 0; cfg->yb = 1;
+      te = 0.295; cfg->tvb_m = 1; cfg->tvb_beta = 0.65;
+      break;
+    case GDF_PROB_CLOUD_SHOCK:
+      cfg->xa = 0; cfg->xb = 2; cfg->ya = 0; cfg->yb = 1;
+      te = 0.6; cfg->tvb_m = 1;
+      bc = GDF_BC_OUTFLOW;
+      break;
+    default:
+      return GDF_ERR_ARG;
+  }
+  cfg->bc_r = cfg->bc_l = cfg->bc_u = cfg->bc_d = bc;
+  if (tend) *tend = te;
+  return GDF_OK;
+}
+
+// init_data (main.f90:534-661) on one rank: the cell projection on modes
+// 1-10 accumulates 0.25*w(i1)*w(j1)*U*phiG over the Gauss points for each
+// mode and divides by mm; the face projection 0.5*w*EzG*B over the edge
+// points, divided by mmE. Ghost slots, ghost face rows/columns and the
+// modes 11-15 stay 0.
+int gdf_p3_init_data(const GdfP3Config* cfg, int32_t problem, double* uh, double* bx, double* by) {
+  if (!cfg || !uh || !bx || !by || cfg->nx < 1 || cfg->ny < 1) return GDF_ERR_ARG;
+  if (problem != GDF_PROB_VORTEX && problem != GDF_PROB_ORSZAG_TANG && problem != GDF_PROB_ROTOR &&
+      problem != GDF_PROB_CLOUD_SHOCK)
+    return GDF_ERR_ARG;
+  using gdf3::BasisP3;
+  using gdf3::NB3;
+  using gdf3::NP3;
+  using gdf3::NQ3;
+  const int Nx = cfg->nx, Ny = cfg->ny;
+  Init P;
+  P.problem = problem;
+  P.g = cfg->gamma;
+  for (int q = 0; q < 8; ++q) P.prm[q] = 0;
+  if (problem == GDF_PROB_ROTOR) {
+    // init4: rho 10 inside r0 = 0.1 with the 0.115 taper, u = (-(y-1/2), x-1/2)/r0,
+    // p 0.5, B1 2.5/sqrt(4 pi) (main.f90:228-305)
+    const double pi = 4 * std::atan(1.0);
+    const double v[8] = {0.5, 0.5, 0.1, 0.115, 10.0, 1.0, 0.5, 2.5 / std::sqrt(4 * pi)};
+    std::memcpy(P.prm, v, sizeof(v));
+  }
+  const double hx = (cfg->xb - cfg->xa) / Nx, hy = (cfg->yb - cfg->ya) / Ny;
+  const double hx1 = 0.5 * hx, hy1 = 0.5 * hy;
+  BasisP3 B;
+  gdf3::build_basis_p3(hx1, hy1, &B);
+  const size_t NX2 = (size_t)Nx + 2, NY2 = (size_t)Ny + 2, plane = NX2 * NY2;
+  std::memset(uh, 0, plane * NP3 * NE * sizeof(double));
+  std::memset(bx, 0, (size_t)(Nx + 1) * NY2 * NB3 * sizeof(double));
+  std::memset(by, 0, NX2 * (size_t)(Ny + 1) * NB3 * sizeof(double));
+  std::vector<double> Xc(Nx + 1), Yc(Ny + 1);
+  for (int i = 1; i <= Nx; ++i) Xc[i] = cfg->xa + (i - 0.5) * hx;
+  for (int j = 1; j <= Ny; ++j) Yc[j] = cfg->ya + (j - 0.5) * hy;
+#pragma omp parallel for schedule(static)
+  for (int j = 1; j <= Ny; ++j)
+    for (int i = 1; i <= Nx; ++i) {
+      double Uq[NG][NG][NE];
+      for (int a = 0; a < NG; ++a)
+        for (int c = 0; c < NG; ++c) P.conserved(Xc[i] + hx1 * kLam[a], Yc[j] + hy1 * kLam[c], Uq[a][c]);
+      for (int d = 0; d < NQ3; ++d)
+        for (int n = 0; n < NE; ++n) {
+          double acc = 0;
+          for (int a = 0; a < NG; ++a)
+            for (int c = 0; c < NG; ++c) acc = acc + 0.25 * kW[a] * kW[c] * Uq[a][c][n] * B.phiG[a][c][d];
+          uh[i + NX2 * (j + NY2 * (d + (size_t)NP3 * n))] = acc / B.mm[d];
+        }
+    }
+  // Bx(0:Nx, 1:Ny) from B1 on the x edges, By(1:Nx, 0:Ny) from B2 on the y edges
+  double Uv[NE];
+  for (int i = 0; i <= Nx; ++i)
+    for (int j = 1; j <= Ny; ++j)
+      for (int d = 0; d < NB3; ++d) {
+        double acc = 0;
+        for (int c = 0; c < NG; ++c) {
+          P.conserved(cfg->xa + i * hx, Yc[j] + hy1 * kLam[c], Uv);
+          acc = acc + 0.5 * kW[c] * B.EzG[c][d] * Uv[5];
+        }
+        bx[i + (size_t)(Nx + 1) * (j + NY2 * d)] = acc / B.mmE[d];
+      }
+  for (int i = 1; i <= Nx; ++i)
+    for (int j = 0; j <= Ny; ++j)
+      for (int d = 0; d < NB3; ++d) {
+        double acc = 0;
+        for (int a = 0; a < NG; ++a) {
+          P.conserved(Xc[i] + hx1 * kLam[a], cfg->ya + j * hy, Uv);
+          acc = acc + 0.5 * kW[a] * B.EzG[a][d] * Uv[6];
+        }
+        by[i + NX2 * (j + (size_t)(Ny + 1) * d)] = acc / B.mmE[d];
+      }
   return GDF_OK;
 }
 

@@ -27,6 +27,7 @@
 // so no FMA is formed, as in a gfortran -O3 build without -march).
 
 #include "../include/gdf.h"
+#include "../include/gdf_p3.h"
 
 #include <cmath>
 #include <cstdint>
@@ -1795,6 +1796,10 @@ void default_params(int problem, double* prm) {
   }
 }
 
+#ifndef GDF_ORACLE_NO_P3
+#include "gdf_oracle_p3.inc"
+#endif
+
 }  // namespace
 
 // ----------------------------------------------------------------- C ABI --
@@ -1964,5 +1969,60 @@ double orc_pow_hxhy(void* h) {
   Oracle& o = *static_cast<Oracle*>(h);
   return std::pow(o.hx * o.hy, 0.75);
 }
+
+#ifndef GDF_ORACLE_NO_P3
+// ------------------------------------------------ the k = 3 variant (P3) --
+void* orc_p3_create(const GdfP3Config* cfg) {
+  if (!cfg || cfg->nx < 1 || cfg->ny < 1) return nullptr;
+  OracleP3* o = new OracleP3();
+  o->setup(*cfg);
+  return o;
+}
+void orc_p3_destroy(void* h) { delete static_cast<OracleP3*>(h); }
+int orc_p3_init_data(void* h, int problem, double* uh, double* bx, double* by) {
+  static_cast<OracleP3*>(h)->init_data(problem, uh, bx, by);
+  return 0;
+}
+int orc_p3_set_bc(void* h, double* uh, double* bx, double* by) {
+  static_cast<OracleP3*>(h)->set_bc(uh, bx, by);
+  return 0;
+}
+int orc_p3_lh(void* h, double* uh, double* bx, double* by, double* du, double* dbx, double* dby) {
+  static_cast<OracleP3*>(h)->Lh(uh, bx, by, du, dbx, dby);
+  return 0;
+}
+int orc_p3_limit(void* h, double* uh, double* bx, double* by, int32_t* flags) {
+  static_cast<OracleP3*>(h)->limit_all(uh, bx, by, flags);
+  return 0;
+}
+int orc_p3_dt(void* h, const double* uh, double* dt) {
+  *dt = static_cast<OracleP3*>(h)->calc_dt(uh);
+  return 0;
+}
+int orc_p3_step(void* h, double* uh, double* bx, double* by, double* t, double tend, double* dt) {
+  static_cast<OracleP3*>(h)->step(uh, bx, by, t, tend, dt);
+  return 0;
+}
+int orc_p3_diagnostics(void* h, const double* uh, double* umax, double* totaldiv) {
+  static_cast<OracleP3*>(h)->diagnostics(uh, umax, totaldiv);
+  return 0;
+}
+// the basis tables, for the orthogonality and trace pins: phiG, phixG,
+// phiyG [25*15 each, (a*5+b)*15+d], phiGR/GL/GU/GD [5*15 each], corner
+// values RU/LU/RD/LD [15 each], mm [15]
+void orc_p3_basis(void* h, double* out) {
+  const OracleP3& o = *static_cast<OracleP3*>(h);
+  double* q = out;
+  for (auto* T : {&o.phiG, &o.phixG, &o.phiyG})
+    for (int a = 0; a < NG; ++a)
+      for (int b = 0; b < NG; ++b)
+        for (int d = 0; d < NP3; ++d) *q++ = (*T)[a][b][d];
+  for (auto* T : {&o.phiGR, &o.phiGL, &o.phiGU, &o.phiGD})
+    for (int g = 0; g < NG; ++g)
+      for (int d = 0; d < NP3; ++d) *q++ = (*T)[g][d];
+  for (auto* T : {&o.phiRU, &o.phiLU, &o.phiRD, &o.phiLD, &o.mm})
+    for (int d = 0; d < NP3; ++d) *q++ = (*T)[d];
+}
+#endif
 
 }  // extern "C"

@@ -13,9 +13,11 @@
 #include <vector>
 
 #include "../include/gdf.h"
+#include "../include/gdf_p3.h"
 
 FlopTally g_flops;
 
+#define GDF_ORACLE_NO_P3 1
 #define double fcnt
 #include "gdf_oracle.cpp"
 #undef double

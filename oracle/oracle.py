@@ -197,3 +197,97 @@ class Oracle:
 
     def reset_flops(self):
         self.L.orc_flops_reset()
+
+
+# ------------------------------------------------ the k = 3 variant (P3) --
+from gdf.p3 import GdfP3Config, p3_new_state  # noqa: E402
+
+
+def _declare_p3(L):
+    if getattr(L, "_p3_declared", False):
+        return L
+    vp, dp, ip = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int32)
+    L.orc_p3_create.restype = vp
+    L.orc_p3_create.argtypes = [C.POINTER(GdfP3Config)]
+    L.orc_p3_destroy.argtypes = [vp]
+    L.orc_p3_init_data.argtypes = [vp, C.c_int, dp, dp, dp]
+    L.orc_p3_set_bc.argtypes = [vp, dp, dp, dp]
+    L.orc_p3_lh.argtypes = [vp, dp, dp, dp, dp, dp, dp]
+    L.orc_p3_limit.argtypes = [vp, dp, dp, dp, ip]
+    L.orc_p3_dt.argtypes = [vp, dp, dp]
+    L.orc_p3_step.argtypes = [vp, dp, dp, dp, dp, C.c_double, dp]
+    L.orc_p3_diagnostics.argtypes = [vp, dp, dp, dp]
+    L.orc_p3_basis.argtypes = [vp, dp]
+    L._p3_declared = True
+    return L
+
+
+class OracleP3:
+    """CPU restatement of MPI_BalsaraP3/main.f90 for one rank."""
+
+    def __init__(self, cfg: GdfP3Config):
+        self.cfg = cfg.copy()
+        self.nx, self.ny = cfg.nx, cfg.ny
+        self.L = _declare_p3(lib())
+        self.h = self.L.orc_p3_create(C.byref(self.cfg))
+        if not self.h:
+            raise ValueError("bad oracle configuration")
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h and getattr(self, "L", None) is not None:
+            self.L.orc_p3_destroy(h)
+            self.h = None
+
+    def state(self):
+        return p3_new_state(self.nx, self.ny)
+
+    def init_data(self, problem: int):
+        uh, bx, by = self.state()
+        self.L.orc_p3_init_data(self.h, problem, dptr(uh), dptr(bx), dptr(by))
+        return uh, bx, by
+
+    def set_bc(self, uh, bx, by):
+        self.L.orc_p3_set_bc(self.h, dptr(uh), dptr(bx), dptr(by))
+
+    def lh(self, uh, bx, by):
+        """Lh (set_bc applied to the given arrays in place): du, dbx, dby."""
+        du, dbx, dby = np.zeros_like(uh), np.zeros_like(bx), np.zeros_like(by)
+        self.L.orc_p3_lh(self.h, dptr(uh), dptr(bx), dptr(by), dptr(du), dptr(dbx), dptr(dby))
+        return du, dbx, dby
+
+    def limit(self, uh, bx, by):
+        """TVB_Limiter then div_free_Balsara in place; per cell the changed
+        variables (bits 0-7) and those given the P3 reconstruction (8-15)."""
+        f = np.zeros((self.ny, self.nx), np.int32)
+        self.L.orc_p3_limit(self.h, dptr(uh), dptr(bx), dptr(by), iptr(f))
+        return f
+
+    def dt(self, uh) -> float:
+        d = C.c_double()
+        self.L.orc_p3_dt(self.h, dptr(uh), C.byref(d))
+        return d.value
+
+    def step(self, uh, bx, by, t: float, tend: float):
+        tt = C.c_double(t)
+        dt = C.c_double()
+        self.L.orc_p3_step(self.h, dptr(uh), dptr(bx), dptr(by), C.byref(tt), tend, C.byref(dt))
+        return tt.value, dt.value
+
+    def diagnostics(self, uh):
+        a, b = C.c_double(), C.c_double()
+        self.L.orc_p3_diagnostics(self.h, dptr(uh), C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def basis(self) -> dict:
+        out = np.zeros(3 * 25 * 15 + 4 * 5 * 15 + 5 * 15)
+        self.L.orc_p3_basis(self.h, dptr(out))
+        o = 0
+        res = {}
+        for k in ("phiG", "phixG", "phiyG"):
+            res[k] = out[o:o + 375].reshape(5, 5, 15); o += 375
+        for k in ("phiGR", "phiGL", "phiGU", "phiGD"):
+            res[k] = out[o:o + 75].reshape(5, 15); o += 75
+        for k in ("phiRU", "phiLU", "phiRD", "phiLD", "mm"):
+            res[k] = out[o:o + 15].copy(); o += 15
+        return res
