@@ -373,6 +373,42 @@ def rotor_extra(gdf, steps: int, hbm_peak, peak_kind, fp64_tflops):
     return out
 
 
+def p3_cloud_extra(gdf, steps: int):
+    """The k = 3 variant on the reference's own configuration of it
+    (MPI_BalsaraP3/main.f90:9: cloud shock 960 x 480, HLL, ten-stage RK4),
+    cell-updates/s over graph replays, beside the oracle on a bounded CPU
+    sample (240 x 120 of the same problem, one step)."""
+    from gdf import p3
+    if os.path.join(REPO, "oracle") not in sys.path:
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+    from oracle import OracleP3
+    cfg, tend = p3.p3_problem_config(gdf.PROB_CLOUD_SHOCK, 960, 480)
+    s = p3.P3Solver(cfg)
+    s.upload(*p3.p3_init_data(cfg, gdf.PROB_CLOUD_SHOCK))
+    s.prepare()
+    s.advance_timed(tend, 3)
+    l0 = s.kernel_launches()
+    _, k, ms = s.advance_timed(tend, steps)
+    out = {"value": 960 * 480 * k / (ms / 1e3), "unit": "cell-updates/s", "ms_per_step": ms / k, "steps": k,
+           "launches_per_step": (s.kernel_launches() - l0) / max(k, 1), "t": s.t,
+           "workload": "cloud shock 960x480 on [0,2]x[0,1], P3 modal DG (15 slots, 84 live), 4-mode face B, "
+                       "HLL, SSP-RK(10,4) CFL 0.75, TVB (M=1) with the P3 reconstruction on every cell, "
+                       "face-B TVB, Balsara div-free; gamma 5/3; state resident"}
+    s.close()
+    cs, _ = p3.p3_problem_config(gdf.PROB_CLOUD_SHOCK, 240, 120)
+    o = OracleP3(cs)
+    uh, bx, by = o.init_data(gdf.PROB_CLOUD_SHOCK)
+    o.limit(uh, bx, by)
+    t0 = time.perf_counter()
+    o.step(uh, bx, by, 0.0, tend)
+    sec = time.perf_counter() - t0
+    from oracle import set_threads
+    out["cpu_baseline"] = {"value": 240 * 120 / sec, "unit": "cell-updates/s", "cores": set_threads(0),
+                           "kind": "port", "sample": "cloud shock 240x120, one RK4 step after the initial "
+                                                     "limiting; oracle/gdf_oracle_p3.inc with OpenMP"}
+    return out
+
+
 def learned_blast512(gdf):
     """Whole runs of the benchmark blast at 512^2 (t = 0.01, every step
     timed) with both methods, and the L1 density difference between them."""
@@ -472,7 +508,8 @@ def run_quick(args):
     --workload ensemble-small  8 instances (64^2..160^2, OT / rotor / blast,
                                HLLD, learned gate) in the persistent kernels
     --workload mlp-train       one epoch of indicator training on 65536
-                               synthetic samples (batch 2048)"""
+                               synthetic samples (batch 2048)
+    --workload p3-cloud        the k = 3 variant's cloud shock, 2n x n cells"""
     import gdf
     gdf.set_device(dist_env()[2])
     w, n = args.workload, args.n
@@ -494,6 +531,19 @@ def run_quick(args):
         _, k, ms = s.advance_timed(tend if w != "rotor" else 1e9, args.steps)
         print(json.dumps({"quick": True, "workload": w, "n": n, "steps": k, "ms_per_step": ms / max(k, 1),
                           "value": n * n * k / (ms / 1e3)}))
+        s.close()
+        return 0
+    if w == "p3-cloud":
+        from gdf import p3
+        cfg, tend = p3.p3_problem_config(gdf.PROB_CLOUD_SHOCK, 2 * n, n)
+        s = p3.P3Solver(cfg, exact=not args.fma)
+        s.upload(*p3.p3_init_data(cfg, gdf.PROB_CLOUD_SHOCK))
+        s.prepare()
+        if args.warmup:
+            s.advance_timed(tend, args.warmup)
+        _, k, ms = s.advance_timed(tend, args.steps)
+        print(json.dumps({"quick": True, "workload": w, "n": [2 * n, n], "steps": k, "ms_per_step": ms / max(k, 1),
+                          "value": 2 * n * n * k / (ms / 1e3)}))
         s.close()
         return 0
     if w == "mlp-train":
@@ -641,7 +691,8 @@ def run_ours(args):
         for name, fn in (("rotor512_plain", lambda: rotor_extra(gdf, 100, hbm_peak, peak_kind, fp64_tflops)),
                          ("blast512_full_run", lambda: learned_blast512(gdf)),
                          ("ensemble", lambda: ensemble_bench(gdf, args.steps)),
-                         ("mlp_train", lambda: mlp_train_bench(gdf))):
+                         ("mlp_train", lambda: mlp_train_bench(gdf)),
+                         ("p3_cloud960", lambda: p3_cloud_extra(gdf, 20))):
             try:
                 extras[name] = fn()
             except Exception as e:   # reported, not fatal: the headline line still prints
@@ -702,7 +753,7 @@ def main():
     ap.add_argument("--fma", action="store_true", help="with --quick: run the FMA build")
     ap.add_argument("--n", type=int, default=512, help="with --quick: cells per side")
     ap.add_argument("--workload", default="blast",
-                    choices=["blast", "blast-plain", "rotor", "ensemble-small", "mlp-train"],
+                    choices=["blast", "blast-plain", "rotor", "ensemble-small", "mlp-train", "p3-cloud"],
                     help="with --quick: what to run")
     args = ap.parse_args()
     if args.quick:

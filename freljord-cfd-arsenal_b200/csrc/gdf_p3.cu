@@ -10,7 +10,7 @@
 // arithmetic. Per stage:
 //   k3_set_bc          set_bc (main.f90:1574-1867) on one block
 //   k3_face<0>, <1>    face traces, fluxes, eigenvalueMm, Riemann solve
-//                      (main.f90:2004-2231) -> Fxh, Fyh
+//                      (main.f90:2006-2230) -> Fxh, Fyh
 //   k3_vertex          corner traces, 2-D vertex solver (:2271-2307) -> EzV
 //   k3_cell<KIND>      volume + surface integrals, mass matrix (:1913-2002,
 //                      :2234-2264), fused with the stage's RK combination
@@ -19,7 +19,7 @@
 //   k3_limit           TVB_Limiter's cell part (:3298-3424) fused with
 //                      div_free_Balsara (:3108-3233)
 // and per step k3_dt_partial + k3_dt_final (calculate_dt, :1469-1541, and
-// the clamp to tend, :1339-1345). A step is captured once as a CUDA graph.
+// the clamp to tend, :1338-1343). A step is captured once as a CUDA graph.
 
 #include <cuda_runtime.h>
 
@@ -84,7 +84,7 @@ struct Scal3 {
 __device__ __forceinline__ long long gtid() { return (long long)blockIdx.x * blockDim.x + threadIdx.x; }
 
 // ------------------------------------------------------------- physics -----
-// Lh's point flux (main.f90:1932-1961, 2021-2183): the first component is
+// Lh's point flux (main.f90:1942-1969, 2021-2164): the first component is
 // rho*u (rho*v), not the momentum itself; K carries the w term on every side.
 template <int DIR>
 __device__ __forceinline__ void flux3(const Side& s, double* F) {
@@ -168,6 +168,21 @@ __device__ __forceinline__ void trace3(const K3& K, const double* __restrict__ U
   }
 }
 
+// the same from a thread's copy of its cell's 84 slots in shared memory
+// (slot s at sm[s * 64])
+__device__ __forceinline__ void trace3s(const double* sm, const double* phi, double* out) {
+#pragma unroll
+  for (int n = 0; n < NE; ++n) {
+    double acc = 0.0;
+#pragma unroll
+    for (int d = 0; d < NP3; ++d) {
+      const int s = slot3(n, d);
+      if (s >= 0) acc = acc + sm[s * 64] * phi[d];
+    }
+    out[n] = acc;
+  }
+}
+
 // column-major 8x8 times vector, summed from zero in column order (MATMUL)
 __device__ __forceinline__ void mv8(const double* A, const double* x, double* y) {
 #pragma unroll
@@ -190,8 +205,8 @@ __device__ __forceinline__ double minmod3(double a, double b, double c, double M
 // --------------------------------------------------------------- set_bc ----
 // Ghost cells: the x ghosts over every row, then the y ghosts over every
 // column (corners from the y pass), i.e. ghost (i, j) takes cell (si, sj)
-// with si, sj the x and y sources. Face fields: Bx ghost rows, By ghost
-// columns.
+// with si, sj the x and y sources. One thread per (slot, ghost cell); then
+// the face fields' ghost rows (Bx) and columns (By), one thread per mode.
 __global__ void __launch_bounds__(128) k3_set_bc(const __grid_constant__ K3 K, double* __restrict__ U,
                                                  double* __restrict__ BX, double* __restrict__ BY,
                                                  const Scal3* __restrict__ sc) {
@@ -199,48 +214,48 @@ __global__ void __launch_bounds__(128) k3_set_bc(const __grid_constant__ K3 K, d
   const long long t = gtid();
   const long long nring = 2LL * K.ny2 + 2LL * K.nx;
   const long long nbx = 2LL * (K.nx + 1), nby = 2LL * (K.ny + 1);
-  if (t < nring) {
+  if (t < nring * NS3) {
+    const int s = (int)(t / nring);
+    const long long g = t - (long long)s * nring;
     int i, j;
-    if (t < 2LL * K.ny2) {
-      j = (int)(t >> 1);
-      i = (t & 1) ? K.nx + 1 : 0;
+    if (g < 2LL * K.ny2) {
+      j = (int)(g >> 1);
+      i = (g & 1) ? K.nx + 1 : 0;
     } else {
-      const long long r = t - 2LL * K.ny2;
+      const long long r = g - 2LL * K.ny2;
       i = (int)(r >> 1) + 1;
       j = (r & 1) ? K.ny + 1 : 0;
     }
-    auto src = [](int q, int n, int lo_periodic, int hi_periodic) {
+    auto src = [](int q, int n, bool lo_periodic, bool hi_periodic) {
       if (q == 0) return lo_periodic ? n : 1;
       if (q == n + 1) return hi_periodic ? 1 : n;
       return q;
     };
     const int si = src(i, K.nx, K.bc_l == GDF_BC_PERIODIC, K.bc_r == GDF_BC_PERIODIC);
     const int sj = src(j, K.ny, K.bc_d == GDF_BC_PERIODIC, K.bc_u == GDF_BC_PERIODIC);
-    const long long c = i + (long long)K.nx2 * j, s0 = si + (long long)K.nx2 * sj;
-#pragma unroll 4
-    for (int s = 0; s < NS3; ++s) U[c + K.plane * s] = U[s0 + K.plane * s];
+    U[i + (long long)K.nx2 * j + K.plane * s] = U[si + (long long)K.nx2 * sj + K.plane * s];
     return;
   }
-  long long r = t - nring;
-  if (r < nbx) {
+  long long r = t - nring * NS3;
+  if (r < nbx * NB3) {
+    const int d = (int)(r / nbx);
+    r -= (long long)d * nbx;
     const int i = (int)(r >> 1);
     const bool up = r & 1;
     const int j = up ? K.ny + 1 : 0;
     const int sj = up ? (K.bc_u == GDF_BC_PERIODIC ? 1 : K.ny) : (K.bc_d == GDF_BC_PERIODIC ? K.ny : 1);
-#pragma unroll
-    for (int d = 0; d < NB3; ++d)
-      BX[i + (long long)(K.nx + 1) * j + K.bxplane * d] = BX[i + (long long)(K.nx + 1) * sj + K.bxplane * d];
+    BX[i + (long long)(K.nx + 1) * j + K.bxplane * d] = BX[i + (long long)(K.nx + 1) * sj + K.bxplane * d];
     return;
   }
-  r -= nbx;
-  if (r < nby) {
+  r -= nbx * NB3;
+  if (r < nby * NB3) {
+    const int d = (int)(r / nby);
+    r -= (long long)d * nby;
     const int j = (int)(r >> 1);
     const bool right = r & 1;
     const int i = right ? K.nx + 1 : 0;
     const int si = right ? (K.bc_r == GDF_BC_PERIODIC ? 1 : K.nx) : (K.bc_l == GDF_BC_PERIODIC ? K.nx : 1);
-#pragma unroll
-    for (int d = 0; d < NB3; ++d)
-      BY[i + (long long)K.nx2 * j + K.byplane * d] = BY[si + (long long)K.nx2 * j + K.byplane * d];
+    BY[i + (long long)K.nx2 * j + K.byplane * d] = BY[si + (long long)K.nx2 * j + K.byplane * d];
   }
 }
 
@@ -293,6 +308,13 @@ __global__ void __launch_bounds__(128) k3_vertex(const __grid_constant__ K3 K, c
 // du of one interior cell: each du(d, n) is one chain of additions in the
 // reference's order (volume points i1 then j1, x faces, y faces, then the
 // mass matrix), held in registers; then the stage's combination.
+// GDF_P3_CELL_SMEM: each thread first copies its cell's 84 slots to shared
+// memory and evaluates the 25 points from there (same values)
+#ifndef GDF_P3_CELL_SMEM
+#define GDF_P3_CELL_SMEM 0
+#endif
+constexpr size_t CELL_SMEM = GDF_P3_CELL_SMEM ? (size_t)NS3 * 64 * sizeof(double) : 0;
+
 template <int KIND>
 __global__ void __launch_bounds__(64) k3_cell(const __grid_constant__ K3 K, double* __restrict__ U,
                                               double* __restrict__ T, double* __restrict__ UII,
@@ -303,18 +325,28 @@ __global__ void __launch_bounds__(64) k3_cell(const __grid_constant__ K3 K, doub
   if (item >= (long long)K.nx * K.ny) return;
   const int i = (int)(item % K.nx) + 1, j = (int)(item / K.nx) + 1;
   const long long c = i + (long long)K.nx2 * j;
+#if GDF_P3_CELL_SMEM
+  extern __shared__ double cell_sm[];
+  double* my = cell_sm + threadIdx.x;
+#pragma unroll 4
+  for (int q = 0; q < NS3; ++q) my[q * 64] = U[c + K.plane * q];
+#endif
   double du[NQ3][NE];
 #pragma unroll
   for (int d = 0; d < NQ3; ++d)
 #pragma unroll
     for (int n = 0; n < NE; ++n) du[d][n] = 0.0;
-  // volume integral (main.f90:1913-2002)
+  // volume integral (main.f90:1924-2003)
 #pragma unroll 1
   for (int a = 0; a < NG; ++a)
 #pragma unroll 1
     for (int b = 0; b < NG; ++b) {
       double uG[NE];
+#if GDF_P3_CELL_SMEM
+      trace3s(my, K.B.phiG[a][b], uG);
+#else
       trace3(K, U, c, K.B.phiG[a][b], uG);
+#endif
       Side s;
       gdf::make_side(K.P, uG, s);
       double Fx[NE], Fy[NE];
@@ -328,7 +360,7 @@ __global__ void __launch_bounds__(64) k3_cell(const __grid_constant__ K3 K, doub
         for (int n = 0; n < NE; ++n) du[d][n] = du[d][n] + wab * (Fx[n] * px + Fy[n] * py);
       }
     }
-  // surface integrals (main.f90:2234-2260): x faces of the cell, then y faces
+  // surface integrals (main.f90:2232-2258): x faces of the cell, then y faces
   {
     const long long fr = i + (long long)(K.nx + 1) * (j - 1), fl = fr - 1;
 #pragma unroll 1
@@ -473,7 +505,7 @@ __global__ void __launch_bounds__(128) k3_bface(const __grid_constant__ K3 K, co
 }
 
 // ------------------------------------------------------- face-B limiting ---
-// main.f90:3427-3478: modes 2-4 of every face rebuilt from the TVB-limited
+// main.f90:3430-3478: modes 2-4 of every face rebuilt from the TVB-limited
 // end differences; mode 1 kept. Reads Fin (ghost rows/columns set), writes Fout.
 __global__ void __launch_bounds__(128) k3_faceb_limit(const __grid_constant__ K3 K, const double* __restrict__ BXin,
                                                       const double* __restrict__ BYin, double* __restrict__ BXout,
@@ -518,7 +550,40 @@ __global__ void __launch_bounds__(128) k3_faceb_limit(const __grid_constant__ K3
 }
 
 // ------------------------------------------------------------- limiter -----
-// TVB_Limiter's cell part (main.f90:3298-3424) on the pre-limit state S
+// One direction of TVB_Limiter's characteristic part: the face slopes X1
+// (mean to + face) and X2 (- face to mean) limited against the mean
+// differences DR, DL in the characteristic variables of the cell mean,
+// back in conserved variables as Y1, Y2. GDF_P3_LIM_SPLIT builds the left
+// eigenvectors for the four products with L and the right ones afterwards
+// (two eigenmatrix evaluations, fewer live registers); the values are the
+// same either way.
+#ifndef GDF_P3_LIM_SPLIT
+#define GDF_P3_LIM_SPLIT 0
+#endif
+__device__ __forceinline__ void char_limit(const Phys& P, int dir, double rho, double u1, double u2, double u3,
+                                           const double* m0, const double* DR, const double* DL, const double* X1,
+                                           const double* X2, double Mh2, double beta, double* R, double* L,
+                                           double* Y1, double* Y2) {
+  double t1[NE], t2[NE], tu[NE], mod1[NE], mod2[NE];
+  gdf::eigenmatrix(P, dir, rho, u1, u2, u3, m0[4], m0[5], m0[6], m0[7], R, L);
+  mv8(L, DR, t1);
+  mv8(L, DL, t2);
+  mv8(L, X1, tu);
+#pragma unroll
+  for (int k = 0; k < NE; ++k) mod1[k] = minmod3(tu[k], t1[k], t2[k], Mh2, beta);
+  if (!GDF_P3_LIM_SPLIT) mv8(R, mod1, Y1);
+  mv8(L, X2, tu);
+#pragma unroll
+  for (int k = 0; k < NE; ++k) mod2[k] = minmod3(tu[k], t1[k], t2[k], Mh2, beta);
+  if (GDF_P3_LIM_SPLIT) {
+    gdf::eigenmatrix(P, dir, rho, u1, u2, u3, m0[4], m0[5], m0[6], m0[7], R, L);
+    mv8(R, mod1, Y1);
+  }
+  mv8(R, mod2, Y2);
+}
+
+
+// TVB_Limiter's cell part (main.f90:3295-3428) on the pre-limit state S
 // (ghosts set) for one interior cell, then div_free_Balsara for it from the
 // limited face fields; writes the cell's 84 slots of D. flags (may be NULL):
 // bits 0-7 changed variables, 8-15 those rebuilt with the P3 reconstruction.
@@ -538,11 +603,10 @@ __global__ void __launch_bounds__(64) k3_limit(const __grid_constant__ K3 K, con
   const double rhoij = m0[0];
   const double u1 = m0[1] / rhoij, u2 = m0[2] / rhoij, u3 = m0[3] / rhoij;
   double R[64], L[64];
-  double DR[NE], DL[NE], X1[NE], X2[NE], t1[NE], t2[NE], tu[NE], mod[NE];
+  double DR[NE], DL[NE], X1[NE], X2[NE];
   double Rm[NE], Lm[NE], Um[NE], Dm[NE];
   unsigned change = 0;
-  // x direction (main.f90:3313-3345)
-  gdf::eigenmatrix(K.P, 0, rhoij, u1, u2, u3, m0[4], m0[5], m0[6], m0[7], R, L);
+  // x direction (main.f90:3312-3345)
 #pragma unroll
   for (int n = 0; n < NE; ++n) {
     DR[n] = at(c + 1, n, 0) - m0[n];
@@ -551,21 +615,11 @@ __global__ void __launch_bounds__(64) k3_limit(const __grid_constant__ K3 K, con
     X1[n] = a2 + (2.0 / 3.0) * a4 + (2.0 / 5.0) * a7;
     X2[n] = a2 - (2.0 / 3.0) * a4 + (2.0 / 5.0) * a7;
   }
-  mv8(L, DR, t1);
-  mv8(L, DL, t2);
-  mv8(L, X1, tu);
-#pragma unroll
-  for (int k = 0; k < NE; ++k) mod[k] = minmod3(tu[k], t1[k], t2[k], K.Mh2x, K.beta);
-  mv8(R, mod, Rm);
-  mv8(L, X2, tu);
-#pragma unroll
-  for (int k = 0; k < NE; ++k) mod[k] = minmod3(tu[k], t1[k], t2[k], K.Mh2x, K.beta);
-  mv8(R, mod, Lm);
+  char_limit(K.P, 0, rhoij, u1, u2, u3, m0, DR, DL, X1, X2, K.Mh2x, K.beta, R, L, Rm, Lm);
 #pragma unroll
   for (int n = 0; n < NE; ++n)
     if (fabs(Rm[n] - X1[n]) > K.change_tol || fabs(Lm[n] - X2[n]) > K.change_tol) change |= 1u << n;
-  // y direction (main.f90:3348-3380)
-  gdf::eigenmatrix(K.P, 1, rhoij, u1, u2, u3, m0[4], m0[5], m0[6], m0[7], R, L);
+  // y direction (main.f90:3347-3380)
 #pragma unroll
   for (int n = 0; n < NE; ++n) {
     DR[n] = at(c + K.nx2, n, 0) - m0[n];
@@ -574,20 +628,11 @@ __global__ void __launch_bounds__(64) k3_limit(const __grid_constant__ K3 K, con
     X1[n] = a3 + (2.0 / 3.0) * a6 + (2.0 / 5.0) * a10;
     X2[n] = a3 - (2.0 / 3.0) * a6 + (2.0 / 5.0) * a10;
   }
-  mv8(L, DR, t1);
-  mv8(L, DL, t2);
-  mv8(L, X1, tu);
-#pragma unroll
-  for (int k = 0; k < NE; ++k) mod[k] = minmod3(tu[k], t1[k], t2[k], K.Mh2y, K.beta);
-  mv8(R, mod, Um);
-  mv8(L, X2, tu);
-#pragma unroll
-  for (int k = 0; k < NE; ++k) mod[k] = minmod3(tu[k], t1[k], t2[k], K.Mh2y, K.beta);
-  mv8(R, mod, Dm);
+  char_limit(K.P, 1, rhoij, u1, u2, u3, m0, DR, DL, X1, X2, K.Mh2y, K.beta, R, L, Um, Dm);
 #pragma unroll
   for (int n = 0; n < NE; ++n)
     if (fabs(Um[n] - X1[n]) > K.change_tol || fabs(Dm[n] - X2[n]) > K.change_tol) change |= 1u << n;
-  // reconstruction (main.f90:3382-3420); the cell B's modes 2 and 3 only
+  // reconstruction (main.f90:3382-3425); the cell B's modes 2 and 3 only
   // feed omega of the divergence-free rebuild below
   unsigned p3 = 0;
   double om_by2 = at(c, 6, 1), om_bx3 = at(c, 5, 2);
@@ -630,7 +675,7 @@ __global__ void __launch_bounds__(64) k3_limit(const __grid_constant__ K3 K, con
     }
   }
   if (flags) flags[item] = (int32_t)(change | (p3 << 8));
-  // div_free_Balsara (main.f90:3119-3226)
+  // div_free_Balsara (main.f90:3119-3225)
   const double omega = om_by2 - om_bx3;
   const long long bxr = i + (long long)(K.nx + 1) * j, bxl = bxr - 1;
   const long long byu = i + (long long)K.nx2 * j, byd = byu - K.nx2;
@@ -720,7 +765,7 @@ __global__ void __launch_bounds__(DT_BS) k3_dt_partial(const __grid_constant__ K
 }
 
 // step 0: dt only (gdf_p3_dt); step 1: RK4's clamp and t update
-// (main.f90:1337-1345) and the stage coefficients dt/6, dt/10
+// (main.f90:1338-1343) and the stage coefficients dt/6, dt/10
 __global__ void __launch_bounds__(DT_BS) k3_dt_final(const __grid_constant__ K3 K, const double* __restrict__ part,
                                                      int nblocks, Scal3* __restrict__ sc, int step) {
   __shared__ double sx[DT_BS], sy[DT_BS];
@@ -895,7 +940,7 @@ int run(GdfP3Handle* h, F&& launch) {
 // set_bc of (S, SX, SY)
 int launch_set_bc(GdfP3Handle* h, double* S, double* SX, double* SY, const Scal3* sc) {
   const K3& K = h->K;
-  const long long n = 2LL * K.ny2 + 2LL * K.nx + 2LL * (K.nx + 1) + 2LL * (K.ny + 1);
+  const long long n = (2LL * K.ny2 + 2LL * K.nx) * NS3 + (2LL * (K.nx + 1) + 2LL * (K.ny + 1)) * NB3;
   return run(h, [&] { k3_set_bc<<<nblk(n, 128), 128, 0, h->st>>>(K, S, SX, SY, sc); });
 }
 
@@ -912,27 +957,27 @@ int launch_lh(GdfP3Handle* h, int kind, const Scal3* sc) {
   return run(h, [&] {
     switch (kind) {
       case KIND_LH:
-        k3_cell<KIND_LH><<<nc, 64, 0, h->st>>>(K, h->U, h->T, h->UII, h->Fxh, h->Fyh, sc);
+        k3_cell<KIND_LH><<<nc, 64, CELL_SMEM, h->st>>>(K, h->U, h->T, h->UII, h->Fxh, h->Fyh, sc);
         k3_bface<KIND_LH><<<nf, 128, 0, h->st>>>(K, h->Fxh, h->Fyh, h->EzV, h->BX, h->BXT, h->BXII, h->BY, h->BYT,
                                                   h->BYII, sc);
         break;
       case KIND_FIRST:
-        k3_cell<KIND_FIRST><<<nc, 64, 0, h->st>>>(K, h->U, h->T, h->UII, h->Fxh, h->Fyh, sc);
+        k3_cell<KIND_FIRST><<<nc, 64, CELL_SMEM, h->st>>>(K, h->U, h->T, h->UII, h->Fxh, h->Fyh, sc);
         k3_bface<KIND_FIRST><<<nf, 128, 0, h->st>>>(K, h->Fxh, h->Fyh, h->EzV, h->BX, h->BXT, h->BXII, h->BY,
                                                      h->BYT, h->BYII, sc);
         break;
       case KIND_STAGE:
-        k3_cell<KIND_STAGE><<<nc, 64, 0, h->st>>>(K, h->U, h->T, h->UII, h->Fxh, h->Fyh, sc);
+        k3_cell<KIND_STAGE><<<nc, 64, CELL_SMEM, h->st>>>(K, h->U, h->T, h->UII, h->Fxh, h->Fyh, sc);
         k3_bface<KIND_STAGE><<<nf, 128, 0, h->st>>>(K, h->Fxh, h->Fyh, h->EzV, h->BX, h->BXT, h->BXII, h->BY,
                                                      h->BYT, h->BYII, sc);
         break;
       case KIND_FIVE:
-        k3_cell<KIND_FIVE><<<nc, 64, 0, h->st>>>(K, h->U, h->T, h->UII, h->Fxh, h->Fyh, sc);
+        k3_cell<KIND_FIVE><<<nc, 64, CELL_SMEM, h->st>>>(K, h->U, h->T, h->UII, h->Fxh, h->Fyh, sc);
         k3_bface<KIND_FIVE><<<nf, 128, 0, h->st>>>(K, h->Fxh, h->Fyh, h->EzV, h->BX, h->BXT, h->BXII, h->BY,
                                                     h->BYT, h->BYII, sc);
         break;
       default:
-        k3_cell<KIND_LAST><<<nc, 64, 0, h->st>>>(K, h->U, h->T, h->UII, h->Fxh, h->Fyh, sc);
+        k3_cell<KIND_LAST><<<nc, 64, CELL_SMEM, h->st>>>(K, h->U, h->T, h->UII, h->Fxh, h->Fyh, sc);
         k3_bface<KIND_LAST><<<nf, 128, 0, h->st>>>(K, h->Fxh, h->Fyh, h->EzV, h->BX, h->BXT, h->BXII, h->BY,
                                                     h->BYT, h->BYII, sc);
         break;

@@ -108,25 +108,29 @@ def test_steps_match_oracle(problem, flux, nx, ny, steps):
     assert np.all(gu[~live] == 0.0)
 
 
-def test_hlld_cloud_shock_breaks_down_identically():
-    """With the HLLD flux (not the reference's choice for this problem, which
-    is HLL) the reference method produces NaN within the first step of the
-    40 x 20 cloud shock (so does HLLC there); the device reproduces the same
-    values and the same NaN slots."""
+def test_hllc_breakdown_is_reproduced():
+    """With the HLLC flux (not the reference's choice for this problem, which
+    is HLL) the reference method divides zero by zero in a y-face star state
+    of the 40 x 20 cloud shock in the second stage of the first step (so does
+    HLLD). Lh of that stage's state: the device gives the same values and
+    NaN in the same slots. (Past this point the runs part ways: NaN's sign
+    bit, which SIGN(1d0, x) reads in minmod, is set on x86 and clear on the
+    GPU.)"""
     cfg, tend = p3_problem_config(gdf.PROB_CLOUD_SHOCK, 40, 20)
-    cfg.flux_type = gdf.FLUX_HLLD
+    cfg.flux_type = gdf.FLUX_HLLC
     o = OracleP3(cfg)
     uh, bx, by = o.init_data(gdf.PROB_CLOUD_SHOCK)
-    s = p3.P3Solver(cfg)
-    s.upload(uh, bx, by)
-    s.prepare()
     o.limit(uh, bx, by)
-    t, dt = o.step(uh, bx, by, 0.0, tend)
-    assert np.isnan(uh[:, :, 1:-1, 1:-1]).any()
-    gt, gdt = s.step(tend)
-    assert gt == t and gdt == dt
-    gu, gx, gy = s.download()
-    assert np.array_equal(gu[:, :, 1:-1, 1:-1], uh[:, :, 1:-1, 1:-1], equal_nan=True)
+    c6 = o.dt(uh) / 6.0
+    du, dbx, dby = o.lh(uh, bx, by)
+    uh, bx, by = uh + c6 * du, bx + c6 * dbx, by + c6 * dby
+    o.limit(uh, bx, by)
+    edu, edbx, edby = o.lh(uh.copy(), bx.copy(), by.copy())
+    assert np.isnan(edu).any()
+    s = p3.P3Solver(cfg)
+    gdu, gdbx, gdby = s.lh(uh, bx, by)
+    assert np.array_equal(gdu, edu, equal_nan=True)
+    assert np.array_equal(gdbx, edbx, equal_nan=True) and np.array_equal(gdby, edby, equal_nan=True)
 
 
 def test_advance_replays_equal_single_steps_and_stop_at_tend():
