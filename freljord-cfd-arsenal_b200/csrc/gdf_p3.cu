@@ -76,6 +76,7 @@ struct K3 {
 
 struct Scal3 {
   double t, dt, tend, c6, c10;
+  double ax, ay;       // the block's largest |u_n +- c_f| (gdf_p3_step_speeds)
   int active;          // 0 once t has reached tend: the step's kernels return at once
   int status;          // bit 0: non-positive density or non-finite energy / dt seen
   long long steps;
@@ -731,7 +732,7 @@ __device__ __forceinline__ double max_skip_nan(double a, double b) { return b > 
 // energy flags sc->status.
 __global__ void __launch_bounds__(DT_BS) k3_dt_partial(const __grid_constant__ K3 K, const double* __restrict__ U,
                                                        double* __restrict__ part, Scal3* __restrict__ sc, int step) {
-  if (step && !sc->active) return;
+  if (step == 1 && !sc->active) return;
   __shared__ double sx[DT_BS], sy[DT_BS];
   const long long item = gtid();
   double ax = 0.0, ay = 0.0;
@@ -764,12 +765,32 @@ __global__ void __launch_bounds__(DT_BS) k3_dt_partial(const __grid_constant__ K
   }
 }
 
-// step 0: dt only (gdf_p3_dt); step 1: RK4's clamp and t update
+// dt from the grid's largest speeds, RK4's clamp and t update
 // (main.f90:1338-1343) and the stage coefficients dt/6, dt/10
+__device__ __forceinline__ void advance_t(const K3& K, double ax, double ay, Scal3* __restrict__ sc) {
+  double dt = K.cfl / (ax / K.hx + ay / K.hy);
+  double t = sc->t;
+  if (t + dt > sc->tend) {
+    dt = sc->tend - t;
+    t = sc->tend;
+  } else {
+    t = t + dt;
+  }
+  if (!(dt > 0.0) || !isfinite(dt)) sc->status |= 1;
+  sc->dt = dt;
+  sc->t = t;
+  sc->c6 = dt / 6.0;
+  sc->c10 = dt / 10.0;
+  sc->active = 1;
+  sc->steps += 1;
+}
+
+// step 0: dt only (gdf_p3_dt); 1: a time step (advance_t); 2: the block's
+// speeds only (gdf_p3_step_speeds, for a maximum over the blocks of a grid)
 __global__ void __launch_bounds__(DT_BS) k3_dt_final(const __grid_constant__ K3 K, const double* __restrict__ part,
                                                      int nblocks, Scal3* __restrict__ sc, int step) {
   __shared__ double sx[DT_BS], sy[DT_BS];
-  if (step && !(sc->t < sc->tend)) {
+  if (step == 1 && !(sc->t < sc->tend)) {
     if (threadIdx.x == 0) sc->active = 0;
     return;
   }
@@ -789,25 +810,25 @@ __global__ void __launch_bounds__(DT_BS) k3_dt_final(const __grid_constant__ K3 
     __syncthreads();
   }
   if (threadIdx.x != 0) return;
-  double dt = K.cfl / (sx[0] / K.hx + sy[0] / K.hy);
-  if (!step) {
-    sc->dt = dt;
+  if (step == 2) {
+    sc->ax = sx[0];
+    sc->ay = sy[0];
     return;
   }
-  double t = sc->t;
-  if (t + dt > sc->tend) {
-    dt = sc->tend - t;
-    t = sc->tend;
-  } else {
-    t = t + dt;
+  if (!step) {
+    sc->dt = K.cfl / (sx[0] / K.hx + sy[0] / K.hy);
+    return;
   }
-  if (!(dt > 0.0) || !isfinite(dt)) sc->status |= 1;
-  sc->dt = dt;
-  sc->t = t;
-  sc->c6 = dt / 6.0;
-  sc->c10 = dt / 10.0;
-  sc->active = 1;
-  sc->steps += 1;
+  advance_t(K, sx[0], sy[0], sc);
+}
+
+// a step of a block from the speeds of the whole grid (gdf_p3_step_begin)
+__global__ void k3_dt_set(const __grid_constant__ K3 K, double ax, double ay, Scal3* __restrict__ sc) {
+  if (!(sc->t < sc->tend)) {
+    sc->active = 0;
+    return;
+  }
+  advance_t(K, ax, ay, sc);
 }
 
 // calculate_umax and calculate_totaldiv's per-cell terms (main.f90:1433-1465,
@@ -882,6 +903,8 @@ int check_config(const GdfP3Config* c) {
     if (b != GDF_BC_PERIODIC && b != GDF_BC_OUTFLOW) return fail(GDF_ERR_ARG, "boundary condition must be 1 or 2");
   if (c->flux_type < 1 || c->flux_type > 4) return fail(GDF_ERR_ARG, "flux_type must be 1..4");
   if (!(c->xb > c->xa) || !(c->yb > c->ya)) return fail(GDF_ERR_ARG, "empty domain");
+  if ((c->nx_global != 0 && c->nx_global < c->nx) || (c->ny_global != 0 && c->ny_global < c->ny))
+    return fail(GDF_ERR_ARG, "a block cannot be larger than its grid (nx_global, ny_global)");
   if (!(c->gamma > 1.0) || !(c->cfl > 0.0) || !(c->tvb_m >= 0.0) || !(c->tvb_beta > 0.0) ||
       !(c->change_tol >= 0.0) || !(c->hlld_eps >= 0.0))
     return fail(GDF_ERR_ARG, "gamma > 1, cfl > 0, tvb_m >= 0, tvb_beta > 0, change_tol >= 0, hlld_eps >= 0");
@@ -901,8 +924,8 @@ void build_k3(const GdfP3Config& c, K3& K) {
   K.bxplane = (long long)(c.nx + 1) * K.ny2;
   K.byplane = (long long)K.nx2 * (c.ny + 1);
   // main.f90:565-568
-  K.hx = (c.xb - c.xa) / c.nx;
-  K.hy = (c.yb - c.ya) / c.ny;
+  K.hx = (c.xb - c.xa) / (c.nx_global > 0 ? c.nx_global : c.nx);
+  K.hy = (c.yb - c.ya) / (c.ny_global > 0 ? c.ny_global : c.ny);
   const double hx1 = 0.5 * K.hx, hy1 = 0.5 * K.hy;
   K.cxs = 0.5 / K.hx;
   K.cys = 0.5 / K.hy;
@@ -944,11 +967,10 @@ int launch_set_bc(GdfP3Handle* h, double* S, double* SX, double* SY, const Scal3
   return run(h, [&] { k3_set_bc<<<nblk(n, 128), 128, 0, h->st>>>(K, S, SX, SY, sc); });
 }
 
-// Lh of U into the stage's outputs (kind)
-int launch_lh(GdfP3Handle* h, int kind, const Scal3* sc) {
+// Lh of U (ghosts as they are) into the stage's outputs (kind)
+int launch_lh_body(GdfP3Handle* h, int kind, const Scal3* sc) {
   const K3& K = h->K;
-  int rc = launch_set_bc(h, h->U, h->BX, h->BY, sc);
-  if (!rc) rc = run(h, [&] { k3_face<0><<<nblk(K.fxplane * NG, 128), 128, 0, h->st>>>(K, h->U, h->Fxh, sc); });
+  int rc = run(h, [&] { k3_face<0><<<nblk(K.fxplane * NG, 128), 128, 0, h->st>>>(K, h->U, h->Fxh, sc); });
   if (!rc) rc = run(h, [&] { k3_face<1><<<nblk(K.fyplane * NG, 128), 128, 0, h->st>>>(K, h->U, h->Fyh, sc); });
   if (!rc) rc = run(h, [&] { k3_vertex<<<nblk(K.vplane, 128), 128, 0, h->st>>>(K, h->U, h->EzV, sc); });
   if (rc) return rc;
@@ -985,10 +1007,16 @@ int launch_lh(GdfP3Handle* h, int kind, const Scal3* sc) {
   });
 }
 
-// TVB_Limiter + div_free_Balsara: (T, BXT, BYT) -> (U, BX, BY)
-int launch_limit(GdfP3Handle* h, const Scal3* sc, int32_t* flags) {
+// set_bc of U, then its Lh
+int launch_lh(GdfP3Handle* h, int kind, const Scal3* sc) {
+  int rc = launch_set_bc(h, h->U, h->BX, h->BY, sc);
+  return rc ? rc : launch_lh_body(h, kind, sc);
+}
+
+// TVB_Limiter + div_free_Balsara: (T, BXT, BYT), ghosts as they are -> (U, BX, BY)
+int launch_limit_body(GdfP3Handle* h, const Scal3* sc, int32_t* flags) {
   const K3& K = h->K;
-  int rc = launch_set_bc(h, h->T, h->BXT, h->BYT, sc);
+  int rc = GDF_OK;
   if (!rc)
     rc = run(h, [&] {
       k3_faceb_limit<<<nblk(K.fxplane + K.fyplane, 128), 128, 0, h->st>>>(K, h->BXT, h->BYT, h->BX, h->BY, sc);
@@ -998,6 +1026,12 @@ int launch_limit(GdfP3Handle* h, const Scal3* sc, int32_t* flags) {
       k3_limit<<<nblk((long long)K.nx * K.ny, 64), 64, 0, h->st>>>(K, h->T, h->U, h->BX, h->BY, flags, sc);
     });
   return rc;
+}
+
+// set_bc of T, then the limiter
+int launch_limit(GdfP3Handle* h, const Scal3* sc, int32_t* flags) {
+  int rc = launch_set_bc(h, h->T, h->BXT, h->BYT, sc);
+  return rc ? rc : launch_limit_body(h, sc, flags);
 }
 
 int launch_dt(GdfP3Handle* h, int step) {
@@ -1291,6 +1325,67 @@ int gdf_p3_advance_timed(GdfP3Handle* h, double tend, int32_t steps, double* t, 
 }
 
 int64_t gdf_p3_kernel_launches(GdfP3Handle* h) { return h ? h->launches : 0; }
+
+// ------------------------------------------------- stage-level control ----
+int gdf_p3_block_arrays(GdfP3Handle* h, double** U, double** T, double** BX, double** BY, double** BXT,
+                        double** BYT) {
+  if (!h) return fail(GDF_ERR_ARG, "null handle");
+  if (U) *U = h->U;
+  if (T) *T = h->T;
+  if (BX) *BX = h->BX;
+  if (BY) *BY = h->BY;
+  if (BXT) *BXT = h->BXT;
+  if (BYT) *BYT = h->BYT;
+  return GDF_OK;
+}
+
+void* gdf_p3_stream(GdfP3Handle* h) { return h ? (void*)h->st : nullptr; }
+
+int gdf_p3_step_speeds(GdfP3Handle* h, double* ax, double* ay) {
+  if (!h || !ax || !ay) return fail(GDF_ERR_ARG, "null argument");
+  if (!h->uploaded) return fail(GDF_ERR_STATE, "no state uploaded");
+  int rc = launch_dt(h, 2);
+  if (rc || (rc = sync_scal(h))) return rc;
+  *ax = h->sc_host->ax;
+  *ay = h->sc_host->ay;
+  return GDF_OK;
+}
+
+int gdf_p3_step_begin(GdfP3Handle* h, double ax, double ay, double tend, double* t, double* dt) {
+  if (!h) return fail(GDF_ERR_ARG, "null handle");
+  if (!h->uploaded) return fail(GDF_ERR_STATE, "no state uploaded");
+  int rc = sync_scal(h);
+  if (rc) return rc;
+  h->sc_host->tend = tend;
+  h->sc_host->active = 1;
+  if ((rc = push_scal(h))) return rc;
+  if ((rc = run(h, [&] { k3_dt_set<<<1, 1, 0, h->st>>>(h->K, ax, ay, h->sc); }))) return rc;
+  if ((rc = sync_scal(h))) return rc;
+  if (t) *t = h->sc_host->t;
+  if (dt) *dt = h->sc_host->dt;
+  return check_status(h);
+}
+
+int gdf_p3_stage_lh(GdfP3Handle* h, int32_t stage) {
+  if (!h) return fail(GDF_ERR_ARG, "null handle");
+  if (stage < 1 || stage > 10) return fail(GDF_ERR_ARG, "stage must be 1..10");
+  const int kind = stage == 1 ? KIND_FIRST : stage == 5 ? KIND_FIVE : stage == 10 ? KIND_LAST : KIND_STAGE;
+  return launch_lh_body(h, kind, h->sc);
+}
+
+int gdf_p3_stage_load_t(GdfP3Handle* h) {
+  if (!h) return fail(GDF_ERR_ARG, "null handle");
+  const K3& K = h->K;
+  CK3(cudaMemcpyAsync(h->T, h->U, (size_t)K.plane * NS3 * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+  CK3(cudaMemcpyAsync(h->BXT, h->BX, bx_bytes(K), cudaMemcpyDeviceToDevice, h->st));
+  CK3(cudaMemcpyAsync(h->BYT, h->BY, by_bytes(K), cudaMemcpyDeviceToDevice, h->st));
+  return GDF_OK;
+}
+
+int gdf_p3_stage_limit(GdfP3Handle* h) {
+  if (!h) return fail(GDF_ERR_ARG, "null handle");
+  return launch_limit_body(h, h->sc, nullptr);
+}
 
 int gdf_p3_lh(GdfP3Handle* h, const double* uh, const double* bx, const double* by, double* du, double* dbx,
               double* dby) {

@@ -15,7 +15,8 @@ module gdf_p3_bind
     integer(c_int32_t) :: bc_r, bc_l, bc_u, bc_d
     integer(c_int32_t) :: flux_type
     real(c_double)     :: gamma, cfl, tvb_m, tvb_beta, hlld_eps, change_tol
-    integer(c_int32_t) :: reserved(4)
+    integer(c_int32_t) :: nx_global, ny_global
+    integer(c_int32_t) :: reserved(2)
   end type gdf_p3_config
 
   interface

@@ -30,7 +30,8 @@ class GdfP3Config(C.Structure):
         ("flux_type", C.c_int32),
         ("gamma", C.c_double), ("cfl", C.c_double), ("tvb_m", C.c_double), ("tvb_beta", C.c_double),
         ("hlld_eps", C.c_double), ("change_tol", C.c_double),
-        ("reserved", C.c_int32 * 4),
+        ("nx_global", C.c_int32), ("ny_global", C.c_int32),
+        ("reserved", C.c_int32 * 2),
     ]
 
     def copy(self) -> "GdfP3Config":
@@ -122,6 +123,15 @@ def _declare(L) -> None:
     L.gdf_p3_limit.argtypes = [vp, dp, dp, dp]
     L.gdf_p3_dt.argtypes = [vp, dp, dp]
     L.gdf_p3_diagnostics.argtypes = [vp, dp, dp]
+    pp = C.POINTER(C.c_void_p)
+    L.gdf_p3_block_arrays.argtypes = [vp, pp, pp, pp, pp, pp, pp]
+    L.gdf_p3_stream.argtypes = [vp]
+    L.gdf_p3_stream.restype = C.c_void_p
+    L.gdf_p3_step_speeds.argtypes = [vp, dp, dp]
+    L.gdf_p3_step_begin.argtypes = [vp, C.c_double, C.c_double, C.c_double, dp, dp]
+    L.gdf_p3_stage_lh.argtypes = [vp, i32]
+    L.gdf_p3_stage_limit.argtypes = [vp]
+    L.gdf_p3_stage_load_t.argtypes = [vp]
     L._gdf_p3_declared = True
 
 
@@ -238,3 +248,32 @@ class P3Solver:
         a, b = C.c_double(), C.c_double()
         _check(self.L, self.L.gdf_p3_diagnostics(self.h, C.byref(a), C.byref(b)))
         return a.value, b.value
+
+    # stage-level control of a block (gdf/p3_dist.py drives it)
+    def block_arrays(self) -> dict:
+        ptrs = [C.c_void_p() for _ in range(6)]
+        _check(self.L, self.L.gdf_p3_block_arrays(self.h, *[C.byref(p) for p in ptrs]))
+        return dict(zip(("U", "T", "BX", "BY", "BXT", "BYT"), (p.value for p in ptrs)))
+
+    def stream(self) -> int:
+        return int(self.L.gdf_p3_stream(self.h) or 0)
+
+    def step_speeds(self):
+        a, b = C.c_double(), C.c_double()
+        _check(self.L, self.L.gdf_p3_step_speeds(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def step_begin(self, ax: float, ay: float, tend: float):
+        t, dt = C.c_double(), C.c_double()
+        _check(self.L, self.L.gdf_p3_step_begin(self.h, ax, ay, tend, C.byref(t), C.byref(dt)))
+        self.t = t.value
+        return t.value, dt.value
+
+    def stage_lh(self, stage: int) -> None:
+        _check(self.L, self.L.gdf_p3_stage_lh(self.h, stage))
+
+    def stage_limit(self) -> None:
+        _check(self.L, self.L.gdf_p3_stage_limit(self.h))
+
+    def stage_load_t(self) -> None:
+        _check(self.L, self.L.gdf_p3_stage_load_t(self.h))

@@ -55,7 +55,11 @@ typedef struct GdfP3Config {
   double tvb_beta;           /* beta of minmod/minmodB (main.f90:3971,3995)   */
   double hlld_eps;           /* HLLD second-stage threshold (:2495): 1e-6     */
   double change_tol;         /* limiter change test (:3330): 1e-13            */
-  int32_t reserved[4];
+  /* a block of a decomposed grid: the cell width is that of the whole grid,
+   * (xb - xa) / nx_global with xa, xb the whole domain (main.f90:565-566
+   * use Nx0, Ny0); 0 for a grid that is one block */
+  int32_t nx_global, ny_global;
+  int32_t reserved[2];
 } GdfP3Config;
 
 typedef struct GdfP3Handle GdfP3Handle;
@@ -96,6 +100,33 @@ int gdf_p3_advance_timed(GdfP3Handle* h, double tend, int32_t steps, double* t, 
 /* Kernel launches issued on this handle so far (graph replays count each
  * node). */
 int64_t gdf_p3_kernel_launches(GdfP3Handle* h);
+
+/*
+ * Stage-level control, for a block of a grid decomposed over several
+ * devices (the reference's MPI ranks, main.f90:8-11): the caller fills the
+ * ghost layers between the calls (set_bc's exchange, main.f90:1574-1867)
+ * and reduces the speeds over the blocks (calculate_dt's MPI maximum,
+ * :1492-1538). One step: gdf_p3_step_speeds on every block, the maxima,
+ * gdf_p3_step_begin, then for stage s = 1..10: fill the ghosts of U, then
+ * gdf_p3_stage_lh(s); unless s == 5: fill the ghosts of T (cells) and of
+ * BXT/BYT (Bx ghost rows, By ghost columns), then gdf_p3_stage_limit.
+ * Device arrays (gdf_p3_block_arrays): U, T as 84 slot planes of
+ * (Nx+2) x (Ny+2) (slot order: modes 1-10 of each variable, then Bx modes 11,
+ * 14 after Bx's ten and By modes 12, 15 after By's ten), BX, BXT, BY, BYT in
+ * the host layout of Bx, By. The calls are asynchronous on the handle's
+ * stream (gdf_p3_stream) except step_speeds and step_begin, which return
+ * values.
+ */
+int gdf_p3_block_arrays(GdfP3Handle* h, double** U, double** T, double** BX, double** BY, double** BXT,
+                        double** BYT);
+void* gdf_p3_stream(GdfP3Handle* h);
+int gdf_p3_step_speeds(GdfP3Handle* h, double* ax, double* ay);
+int gdf_p3_step_begin(GdfP3Handle* h, double ax, double ay, double tend, double* t, double* dt);
+int gdf_p3_stage_lh(GdfP3Handle* h, int32_t stage);
+int gdf_p3_stage_limit(GdfP3Handle* h);
+/* T = U, BXT = BX, BYT = BY: with a ghost fill of T and gdf_p3_stage_limit,
+ * the block's part of gdf_p3_prepare */
+int gdf_p3_stage_load_t(GdfP3Handle* h);
 
 /* The three calls below take a state from the caller, which replaces the
  * handle's resident state. */
