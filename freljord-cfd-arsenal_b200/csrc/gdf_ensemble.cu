@@ -919,7 +919,7 @@ int gdf_ens_set_indicator(GdfEnsemble* e, GdfMlp* m, float t_lo, float t_hi) {
   std::vector<EnsInst> hi(e->n);
   for (int i = 0; i < e->n; ++i) {
     EnsInst& d = e->in[i].d;
-    if (!d.QM) ECK(cudaMalloc((void**)&d.QM, (size_t)18 * e->in[i].K.plane * sizeof(float)));
+    if (!d.QM) ECK(cudaMalloc((void**)&d.QM, (size_t)QMODES * e->in[i].K.plane * sizeof(float)));
     if (!d.pnet) ECK(cudaMalloc((void**)&d.pnet, (size_t)e->in[i].K.nx * e->in[i].K.ny * sizeof(float)));
     hi[i] = d;
   }

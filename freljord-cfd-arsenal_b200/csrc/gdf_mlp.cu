@@ -68,6 +68,8 @@ struct FwdSmem {
   float red_b1[4][MLP_H], red_b2[4][MLP_H], red_w3[4][MLP_H];
 };
 
+static_assert(GDF_MLP_NPARAM == MLP_NPARAM, "gdf.h and gdf_mlp.cuh disagree on the parameter count");
+
 __global__ void k_mlp_sync(const float* __restrict__ P, MlpDev* __restrict__ D) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < MLP_H * MLP_INP) {

@@ -322,8 +322,9 @@ def main(argv=None):
     ap = argparse.ArgumentParser(prog="python -m gdf.indicator")
     sub = ap.add_subparsers(dest="cmd", required=True)
     t = sub.add_parser("train")
-    t.add_argument("--n", type=int, default=256)
-    t.add_argument("--seeds", type=int, default=32)
+    t.add_argument("--n", type=int, nargs="+", default=[256],
+                   help="grid sides; with several, --seeds gives the seed count of each")
+    t.add_argument("--seeds", type=int, nargs="+", default=[32])
     t.add_argument("--samples-per-run", type=int, default=8)
     t.add_argument("--keep", type=float, default=0.2)
     t.add_argument("--epochs", type=int, default=40)
@@ -341,7 +342,14 @@ def main(argv=None):
     log = lambda m: print(m, flush=True)  # noqa: E731
     if a.cmd == "train":
         t0 = time.time()
-        X, y = collect(a.n, range(a.seeds), a.samples_per_run, a.keep, log=log)
+        if len(a.seeds) != len(a.n):
+            raise SystemExit("--seeds needs one count per --n")
+        parts = []
+        for k, (n, ns) in enumerate(zip(a.n, a.seeds)):
+            # disjoint training seeds per resolution (held-out seeds are 1000+)
+            parts.append(collect(n, range(100 * k, 100 * k + ns), a.samples_per_run, a.keep, log=log))
+        X = np.concatenate([p[0] for p in parts])
+        y = np.concatenate([p[1] for p in parts])
         log(f"collected {len(y)} cells ({int(y.sum())} positive) in {time.time() - t0:.1f} s")
         net, t_lo, t_hi, rep = train(X, y, epochs=a.epochs, log=log)
         rep.update({"grid": a.n, "train_seeds": a.seeds, "samples_per_run": a.samples_per_run, "keep": a.keep})
