@@ -554,35 +554,35 @@ __global__ void __launch_bounds__(128) k3_faceb_limit(const __grid_constant__ K3
 // One direction of TVB_Limiter's characteristic part: the face slopes X1
 // (mean to + face) and X2 (- face to mean) limited against the mean
 // differences DR, DL in the characteristic variables of the cell mean,
-// back in conserved variables as Y1, Y2. GDF_P3_LIM_SPLIT builds the left
-// eigenvectors for the four products with L and the right ones afterwards
-// (two eigenmatrix evaluations, fewer live registers); the values are the
-// same either way.
-#ifndef GDF_P3_LIM_SPLIT
-#define GDF_P3_LIM_SPLIT 0
-#endif
+// back in conserved variables as Y1, Y2. The left eigenvectors are built
+// and used in the four products with L (main.f90:3319-3321, 3337), then
+// the right ones for the two products with R: one 8x8 matrix live at a
+// time, the same products and sums as with both (this eigenmatrix has no
+// identity fallback that would tie R to L).
 __device__ __forceinline__ void char_limit(const Phys& P, int dir, double rho, double u1, double u2, double u3,
                                            const double* m0, const double* DR, const double* DL, const double* X1,
-                                           const double* X2, double Mh2, double beta, double* R, double* L,
-                                           double* Y1, double* Y2) {
-  double t1[NE], t2[NE], tu[NE], mod1[NE], mod2[NE];
-  gdf::eigenmatrix(P, dir, rho, u1, u2, u3, m0[4], m0[5], m0[6], m0[7], R, L);
-  mv8(L, DR, t1);
-  mv8(L, DL, t2);
-  mv8(L, X1, tu);
+                                           const double* X2, double Mh2, double beta, double* Y1, double* Y2) {
+  gdf::EigFrame f;
+  gdf::eigen_frame(P, dir, rho, u1, u2, u3, m0[4], m0[5], m0[6], m0[7], f);
+  double mod1[NE], mod2[NE];
+  {
+    double L[64], t1[NE], t2[NE], tu1[NE], tu2[NE];
+    gdf::eigen_left(dir, f, rho, u1, u2, u3, m0[5], m0[6], m0[7], L);
+    mv8(L, DR, t1);
+    mv8(L, DL, t2);
+    mv8(L, X1, tu1);
+    mv8(L, X2, tu2);
 #pragma unroll
-  for (int k = 0; k < NE; ++k) mod1[k] = minmod3(tu[k], t1[k], t2[k], Mh2, beta);
-  if (!GDF_P3_LIM_SPLIT) mv8(R, mod1, Y1);
-  mv8(L, X2, tu);
-#pragma unroll
-  for (int k = 0; k < NE; ++k) mod2[k] = minmod3(tu[k], t1[k], t2[k], Mh2, beta);
-  if (GDF_P3_LIM_SPLIT) {
-    gdf::eigenmatrix(P, dir, rho, u1, u2, u3, m0[4], m0[5], m0[6], m0[7], R, L);
-    mv8(R, mod1, Y1);
+    for (int k = 0; k < NE; ++k) {
+      mod1[k] = minmod3(tu1[k], t1[k], t2[k], Mh2, beta);
+      mod2[k] = minmod3(tu2[k], t1[k], t2[k], Mh2, beta);
+    }
   }
+  double R[64];
+  gdf::eigen_right(dir, f, rho, u1, u2, u3, m0[5], m0[6], m0[7], R);
+  mv8(R, mod1, Y1);
   mv8(R, mod2, Y2);
 }
-
 
 // TVB_Limiter's cell part (main.f90:3295-3428) on the pre-limit state S
 // (ghosts set) for one interior cell, then div_free_Balsara for it from the
@@ -603,7 +603,6 @@ __global__ void __launch_bounds__(64) k3_limit(const __grid_constant__ K3 K, con
   for (int n = 0; n < NE; ++n) m0[n] = at(c, n, 0);
   const double rhoij = m0[0];
   const double u1 = m0[1] / rhoij, u2 = m0[2] / rhoij, u3 = m0[3] / rhoij;
-  double R[64], L[64];
   double DR[NE], DL[NE], X1[NE], X2[NE];
   double Rm[NE], Lm[NE], Um[NE], Dm[NE];
   unsigned change = 0;
@@ -616,7 +615,7 @@ __global__ void __launch_bounds__(64) k3_limit(const __grid_constant__ K3 K, con
     X1[n] = a2 + (2.0 / 3.0) * a4 + (2.0 / 5.0) * a7;
     X2[n] = a2 - (2.0 / 3.0) * a4 + (2.0 / 5.0) * a7;
   }
-  char_limit(K.P, 0, rhoij, u1, u2, u3, m0, DR, DL, X1, X2, K.Mh2x, K.beta, R, L, Rm, Lm);
+  char_limit(K.P, 0, rhoij, u1, u2, u3, m0, DR, DL, X1, X2, K.Mh2x, K.beta, Rm, Lm);
 #pragma unroll
   for (int n = 0; n < NE; ++n)
     if (fabs(Rm[n] - X1[n]) > K.change_tol || fabs(Lm[n] - X2[n]) > K.change_tol) change |= 1u << n;
@@ -629,7 +628,7 @@ __global__ void __launch_bounds__(64) k3_limit(const __grid_constant__ K3 K, con
     X1[n] = a3 + (2.0 / 3.0) * a6 + (2.0 / 5.0) * a10;
     X2[n] = a3 - (2.0 / 3.0) * a6 + (2.0 / 5.0) * a10;
   }
-  char_limit(K.P, 1, rhoij, u1, u2, u3, m0, DR, DL, X1, X2, K.Mh2y, K.beta, R, L, Um, Dm);
+  char_limit(K.P, 1, rhoij, u1, u2, u3, m0, DR, DL, X1, X2, K.Mh2y, K.beta, Um, Dm);
 #pragma unroll
   for (int n = 0; n < NE; ++n)
     if (fabs(Um[n] - X1[n]) > K.change_tol || fabs(Dm[n] - X2[n]) > K.change_tol) change |= 1u << n;

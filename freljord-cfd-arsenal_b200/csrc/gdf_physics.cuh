@@ -518,22 +518,36 @@ GDF_HD void tangent(int dir, double B1, double B2, double B3, double& t1, double
   t3 = tp3 / nrm;
 }
 
-GDF_HD void eigenmatrix(const Phys& P, int dir, double rho, double u1, double u2, double u3, double E, double B1,
-                        double B2, double B3, double* R, double* L) {
-  const double gm = P.gflux;
-  const double g1 = gm - 1.0;
+// The quantities both eigenvector sets of eigenmatrix.f90 start from: the
+// pressure (:21), the tangent t of compute_t_vector (:411-433) and n x t.
+struct EigFrame {
+  double gm, g1, p, t1, t2, t3, TxN1, TxN2, TxN3;
+};
+GDF_HD void eigen_frame(const Phys& P, int dir, double rho, double u1, double u2, double u3, double E, double B1,
+                        double B2, double B3, EigFrame& f) {
+  f.gm = P.gflux;
+  f.g1 = f.gm - 1.0;
   const double kin = sq(u1) + sq(u2) + sq(u3);
-  const double p = P.eig_p_typo ? g1 * (E - 0.5 * kin - 0.5 * (sq(B1) + sq(B2) + sq(B3)))
-                                : g1 * (E - 0.5 * rho * kin - 0.5 * (sq(B1) + sq(B2) + sq(B3)));
-  double t1, t2, t3;
-  tangent(dir, B1, B2, B3, t1, t2, t3);
+  f.p = P.eig_p_typo ? f.g1 * (E - 0.5 * kin - 0.5 * (sq(B1) + sq(B2) + sq(B3)))
+                     : f.g1 * (E - 0.5 * rho * kin - 0.5 * (sq(B1) + sq(B2) + sq(B3)));
+  tangent(dir, B1, B2, B3, f.t1, f.t2, f.t3);
   // normal components: n_d = 1, others 0
   // TxN = n x t rotated as in the reference: TxN1 = n3 t2 - n2 t3, ...
-  const double TxN1 = dir == 0 ? 0.0 : -t3;
-  const double TxN2 = dir == 0 ? t3 : 0.0;
-  const double TxN3 = dir == 0 ? -t2 : t1;
+  f.TxN1 = dir == 0 ? 0.0 : -f.t3;
+  f.TxN2 = dir == 0 ? f.t3 : 0.0;
+  f.TxN3 = dir == 0 ? -f.t2 : f.t1;
+}
 
-  // ---- right eigenvectors (eigenmatrix.f90:21-180)
+#define GDF_EIG_UNPACK                                                   \
+  const double gm = f.gm, g1 = f.g1, p = f.p, t1 = f.t1, t2 = f.t2, t3 = f.t3; \
+  const double TxN1 = f.TxN1, TxN2 = f.TxN2, TxN3 = f.TxN3;              \
+  (void)gm; (void)g1; (void)p; (void)t1; (void)t2; (void)t3;            \
+  (void)TxN1; (void)TxN2; (void)TxN3;
+
+// right eigenvectors (eigenmatrix.f90:21-180), column-major R[r + 8*c]
+GDF_HD void eigen_right(int dir, const EigFrame& f, double rho, double u1, double u2, double u3, double B1, double B2,
+                        double B3, double* R) {
+  GDF_EIG_UNPACK
   {
     const double rhosq = sqrt(fabs(rho));
     const double a2 = fabs(gm * p / rho);
@@ -634,8 +648,12 @@ GDF_HD void eigenmatrix(const Phys& P, int dir, double rho, double u1, double u2
       R[7 + 8 * m] = dvz<false>(ru[7][m], g1);
     }
   }
+}
 
-  // ---- left eigenvectors (eigenmatrix.f90:185-394)
+// left eigenvectors (eigenmatrix.f90:185-394), column-major L[r + 8*c]
+GDF_HD void eigen_left(int dir, const EigFrame& f, double rho, double u1, double u2, double u3, double B1, double B2,
+                       double B3, double* L) {
+  GDF_EIG_UNPACK
   {
     const double rhosq = sqrt(rho);
     const double a2 = fabs(gm * p / rho);
@@ -769,6 +787,14 @@ GDF_HD void eigenmatrix(const Phys& P, int dir, double rho, double u1, double u2
       L[m + 8 * 7] = l[7] * g1 - B3 * l[4] * g12;
     }
   }
+}
+
+GDF_HD void eigenmatrix(const Phys& P, int dir, double rho, double u1, double u2, double u3, double E, double B1,
+                        double B2, double B3, double* R, double* L) {
+  EigFrame f;
+  eigen_frame(P, dir, rho, u1, u2, u3, E, B1, B2, B3, f);
+  eigen_right(dir, f, rho, u1, u2, u3, B1, B2, B3, R);
+  eigen_left(dir, f, rho, u1, u2, u3, B1, B2, B3, L);
   if (P.eig_identity) {
     double sr = 0, sl = 0;
 #pragma unroll
