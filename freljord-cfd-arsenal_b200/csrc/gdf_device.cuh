@@ -1004,7 +1004,72 @@ __device__ __forceinline__ void lim_tvb_p1(const Consts& K, const double* __rest
   word |= (int32_t)change;
 }
 
-template <bool ROLLED = false>
+// One direction of TVB_Limiter_P2.f90's characteristic part
+// (:24-55 x, :57-90 y): the face slopes Dp (mean to + face) and Dm (- face
+// to mean) limited against the mean differences DR, DL in the
+// characteristic variables of the cell mean (minmod with the bound Mh2),
+// back in conserved variables as Yp, Ym. The left eigenvectors are built
+// and used in the four products with L before the right ones are built, so
+// one 8x8 matrix is live at a time; the products and sums are those of
+// eigenmatrix's R and L. With the identity fallback of eigenmatrix.f90:
+// 397-404 (either matrix summing above 1e4 in absolute value) both
+// matrices are the identity, and the products are taken with it.
+__device__ __forceinline__ void char_limit_dir(const Consts& K, int dir, double rho, double u1, double u2,
+                                               double u3, double E, double B1, double B2, double B3,
+                                               const double* DR, const double* DL, const double* Dp,
+                                               const double* Dm, double Mh2, double* Yp, double* Ym) {
+  EigFrame f;
+  eigen_frame(K.P, dir, rho, u1, u2, u3, E, B1, B2, B3, f);
+  double t1[NE], t2[NE], tp[NE], tm[NE];
+  double sl = 0.0;
+  {
+    double L[64];
+    eigen_left(dir, f, rho, u1, u2, u3, B1, B2, B3, L);
+    if (K.P.eig_identity) {
+#pragma unroll
+      for (int q = 0; q < 64; ++q) sl = sl + fabs(L[q]);
+    }
+    matvec8(L, DR, t1);
+    matvec8(L, DL, t2);
+    matvec8(L, Dp, tp);
+    matvec8(L, Dm, tm);
+  }
+  double R[64];
+  eigen_right(dir, f, rho, u1, u2, u3, B1, B2, B3, R);
+  if (K.P.eig_identity) {
+    double sr = 0.0;
+#pragma unroll
+    for (int q = 0; q < 64; ++q) sr = sr + fabs(R[q]);
+    if (sr > 1e4 || sl > 1e4) {
+#pragma unroll
+      for (int q = 0; q < 64; ++q) R[q] = (q % 9 == 0) ? 1.0 : 0.0;
+      matvec8(R, DR, t1);
+      matvec8(R, DL, t2);
+      matvec8(R, Dp, tp);
+      matvec8(R, Dm, tm);
+    }
+  }
+  double mod[NE];
+#pragma unroll
+  for (int k = 0; k < NE; ++k) mod[k] = minmod1(tp[k], t1[k], t2[k], Mh2);
+  matvec8(R, mod, Yp);
+#pragma unroll
+  for (int k = 0; k < NE; ++k) mod[k] = minmod1(tm[k], t1[k], t2[k], Mh2);
+  matvec8(R, mod, Ym);
+}
+
+// STREAM: lim_tvb through char_limit_dir (one eigenvector matrix live at a
+// time) instead of both matrices at once; same values. GDF_TVB_STREAM=1
+// gives it to the second limiter pass: k_limit_tvb 0.50 against 0.60 ms
+// per launch on the developed rotor 512^2, but the blast 2048^2 step, which
+// never launches that kernel, measured 46.3 against 45.5 ms with it (three
+// A/B pairs, equal hashes; a build of the same source by another route
+// measured the same), so the product keeps it off.
+#ifndef GDF_TVB_STREAM
+#define GDF_TVB_STREAM 0
+#endif
+
+template <bool ROLLED = false, bool STREAM = false>
 __device__ __forceinline__ void lim_tvb(const Consts& K, const double* __restrict__ S, long long c,
                                         double (*m)[NP], int32_t& word) {
   if (K.tvb_p1) {
@@ -1020,6 +1085,33 @@ __device__ __forceinline__ void lim_tvb(const Consts& K, const double* __restric
     double DR[NE], DL[NE], Dp[NE], Dm[NE], t1[NE], t2[NE], tu[NE], mod[NE];
     double Rp[NE], Rm[NE], Up[NE], Um[NE];
     unsigned change = 0;
+    if (!ROLLED && STREAM) {
+#pragma unroll
+      for (int n = 0; n < NE; ++n) {
+        DR[n] = S[c + 1 + pl * (10 * n)] - m[n][0];
+        DL[n] = m[n][0] - S[c - 1 + pl * (10 * n)];
+        Dp[n] = m[n][1] + c23 * m[n][3];
+        Dm[n] = m[n][1] - c23 * m[n][3];
+      }
+      char_limit_dir(K, 0, rhoij, u1, u2, u3, Eij, B1, B2, B3, DR, DL, Dp, Dm, K.Mh2x, Rp, Rm);
+#pragma unroll
+      for (int d = 0; d < NE; ++d)
+        if (fabs(Rp[d] - Dp[d]) > 1e-6 || fabs(Rm[d] - Dm[d]) > 1e-6) change |= 1u << d;
+#pragma unroll
+      for (int n = 0; n < NE; ++n) {
+        DR[n] = S[c + K.nx2 + pl * (10 * n)] - m[n][0];
+        DL[n] = m[n][0] - S[c - K.nx2 + pl * (10 * n)];
+        Dp[n] = m[n][2] + c23 * m[n][5];
+        Dm[n] = m[n][2] - c23 * m[n][5];
+      }
+      if (K.eig_y_zero_w)
+        char_limit_dir(K, 1, rhoij, u1, u2, 0.0, Eij, B1, B2, 0.0, DR, DL, Dp, Dm, K.Mh2y, Up, Um);
+      else
+        char_limit_dir(K, 1, rhoij, u1, u2, u3, Eij, B1, B2, B3, DR, DL, Dp, Dm, K.Mh2y, Up, Um);
+#pragma unroll
+      for (int d = 0; d < NE; ++d)
+        if (fabs(Up[d] - Dp[d]) > 1e-6 || fabs(Um[d] - Dm[d]) > 1e-6) change |= 1u << d;
+    } else {
     // x direction
     if (ROLLED) eigenmatrix_call(K.P, 0, rhoij, u1, u2, u3, Eij, B1, B2, B3, R, L);
     else eigenmatrix(K.P, 0, rhoij, u1, u2, u3, Eij, B1, B2, B3, R, L);
@@ -1076,6 +1168,7 @@ __device__ __forceinline__ void lim_tvb(const Consts& K, const double* __restric
 #pragma unroll
     for (int d = 0; d < NE; ++d)
       if (fabs(Um[d] - Dm[d]) > 1e-6) change |= 1u << d;
+    }
 #pragma unroll
     for (int n = 0; n < NE; ++n) {
       if (change & (1u << n)) {
@@ -1203,7 +1296,7 @@ __device__ __forceinline__ void limit_tvb_item(const Consts& K, const double* __
 #pragma unroll
     for (int d = 0; d < NP; ++d) m[n][d] = live_mode(n, d) ? S[c + pl * (d + 10 * n)] : 0.0;
   int32_t word = K.detector != GDF_DETECT_ALL ? (1 << 24) : 0;
-  lim_tvb<GDF_TVB_ROLLED>(K, S, c, m, word);
+  lim_tvb<GDF_TVB_ROLLED, GDF_TVB_STREAM != 0>(K, S, c, m, word);
   lim_finish(K, D, BX, BY, flags, stage, divfree, sc, item, i, j, c, m, word);
 }
 
