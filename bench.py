@@ -409,6 +409,45 @@ def p3_cloud_extra(gdf, steps: int):
     return out
 
 
+def cy_ot_extra(gdf, steps: int):
+    """The cylindrical variant (MHD_GDF_cy3D_0421/) on the reference's own
+    configuration (com.txt:1 Nr = Nz = 192, Lphi = 1: two phi planes; the
+    cylindrical Orszag-Tang vortex of init3.txt, HLL, RK3 CFL 0.2) and on a
+    1024^2 grid of the same problem, cell-plane updates/s over graph
+    replays, beside the oracle on the 192^2 case (one step)."""
+    from gdf import cy
+    if os.path.join(REPO, "oracle") not in sys.path:
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+    from oracle import OracleCy, set_threads
+    out = {}
+    for n in (192, 1024):
+        cfg, tend = cy.cy_problem_config(cy.CY_ORSZAG_TANG, n, n, 1)
+        s = cy.CySolver(cfg)
+        s.upload(*cy.cy_init_data(cfg, cy.CY_ORSZAG_TANG))
+        s.prepare()
+        s.advance_timed(tend, 3)
+        l0 = s.kernel_launches()
+        _, k, ms = s.advance_timed(tend, steps)
+        out[f"ot{n}"] = {"value": n * n * 2 * k / (ms / 1e3), "unit": "cell-plane-updates/s",
+                         "ms_per_step": ms / k, "steps": k,
+                         "launches_per_step": (s.kernel_launches() - l0) / max(k, 1)}
+        s.close()
+    out["workload"] = ("cylindrical Orszag-Tang (init3.txt) on r in [6pi, 8pi], z in [0, 2pi], 2 phi planes, "
+                       "P2 modal DG (10 slots, 54 live), 3-mode face r*B, HLL, SSP-RK3 CFL 0.2, characteristic "
+                       "TVB (M=10) on every cell, face-B minmod, Balsara div-free; gamma 5/3; state resident")
+    cfg, tend = cy.cy_problem_config(cy.CY_ORSZAG_TANG, 192, 192, 1)
+    o = OracleCy(cfg)
+    uh, br, bz = o.init_data(cy.CY_ORSZAG_TANG)
+    o.limit(uh, br, bz)
+    t0 = time.perf_counter()
+    o.step(uh, br, bz, 0.0, tend)
+    sec = time.perf_counter() - t0
+    out["cpu_baseline"] = {"value": 192 * 192 * 2 / sec, "unit": "cell-plane-updates/s", "cores": set_threads(0),
+                           "kind": "port", "sample": "the 192^2 x 2 reference configuration, one RK3 step after "
+                                                     "the initial limiting; oracle/gdf_oracle_cy.inc with OpenMP"}
+    return out
+
+
 def learned_blast512(gdf):
     """Whole runs of the benchmark blast at 512^2 (t = 0.01, every step
     timed) with both methods, and the L1 density difference between them."""
@@ -692,7 +731,8 @@ def run_ours(args):
                          ("blast512_full_run", lambda: learned_blast512(gdf)),
                          ("ensemble", lambda: ensemble_bench(gdf, args.steps)),
                          ("mlp_train", lambda: mlp_train_bench(gdf)),
-                         ("p3_cloud960", lambda: p3_cloud_extra(gdf, 20))):
+                         ("p3_cloud960", lambda: p3_cloud_extra(gdf, 20)),
+                         ("cy_orszag_tang", lambda: cy_ot_extra(gdf, 40))):
             try:
                 extras[name] = fn()
             except Exception as e:   # reported, not fatal: the headline line still prints

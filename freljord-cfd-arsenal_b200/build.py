@@ -32,11 +32,14 @@ PEAK_SRC = os.path.join(CSRC, "gdf_peak.cu")
 INIT_SRC = os.path.join(CSRC, "gdf_init.cu")
 MLPTC_SRC = os.path.join(CSRC, "gdf_mlp_tc.cu")
 P3_SRC = os.path.join(CSRC, "gdf_p3.cu")
+CY_SRC = os.path.join(CSRC, "gdf_cy.cu")
 HOST_SRC = os.path.join(CSRC, "gdf_host.cpp")
 IO_SRC = os.path.join(CSRC, "gdf_io.cpp")
+CYHOST_SRC = os.path.join(CSRC, "gdf_cy_host.cpp")
 HEADERS = [os.path.join(CSRC, f) for f in ("gdf_physics.cuh", "gdf_kernels.cuh", "gdf_device.cuh",
                                                          "gdf_mlp.cuh", "gdf_p3_basis.h")] + [
-    os.path.join(REPO, "include", "gdf.h"), os.path.join(REPO, "include", "gdf_p3.h")]
+    os.path.join(REPO, "include", "gdf.h"), os.path.join(REPO, "include", "gdf_p3.h"),
+    os.path.join(REPO, "include", "gdf_cy.h")]
 
 
 def _nvcc() -> str:
@@ -69,8 +72,9 @@ def build(verbose: bool = False, jobs: int | None = None) -> dict:
     nvcc = _nvcc()
     host_o = os.path.join(BUILD, "gdf_host.o")
     io_o = os.path.join(BUILD, "gdf_io.o")
+    cyh_o = os.path.join(BUILD, "gdf_cy_host.o")
     cmds = []
-    for src, obj in ((HOST_SRC, host_o), (IO_SRC, io_o)):
+    for src, obj in ((HOST_SRC, host_o), (IO_SRC, io_o), (CYHOST_SRC, cyh_o)):
         if _stale(obj, [src] + HEADERS):
             cmds.append([HOST_CXX, "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-march=x86-64", "-fopenmp",
                          "-c", src, "-o", obj])
@@ -78,7 +82,7 @@ def build(verbose: bool = False, jobs: int | None = None) -> dict:
     for name, flags in (("libgdf_b200.so", ["--fmad=false", "-DGDF_EXACT=1"]),
                         ("libgdf_b200_fma.so", ["--fmad=true"])):
         objs = []
-        for src in (KERNEL_SRC, MLP_SRC, ENS_SRC, PEAK_SRC, INIT_SRC, MLPTC_SRC, P3_SRC):
+        for src in (KERNEL_SRC, MLP_SRC, ENS_SRC, PEAK_SRC, INIT_SRC, MLPTC_SRC, P3_SRC, CY_SRC):
             obj = os.path.join(BUILD, name.replace(".so", "") + "_" + os.path.basename(src).replace(".cu", ".o"))
             if _stale(obj, [src] + HEADERS):
                 cmd = [nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17", *flags,
@@ -96,8 +100,8 @@ def build(verbose: bool = False, jobs: int | None = None) -> dict:
     out = {}
     for name, objs in libs:
         so = os.path.join(LIB, name)
-        if _stale(so, objs + [host_o, io_o]):
-            _run([nvcc, *ARCH, "-shared", "-o", so, *objs, host_o, io_o, "-Xcompiler", "-fopenmp", "-lgomp"])
+        if _stale(so, objs + [host_o, io_o, cyh_o]):
+            _run([nvcc, *ARCH, "-shared", "-o", so, *objs, host_o, io_o, cyh_o, "-Xcompiler", "-fopenmp", "-lgomp"])
         out[name] = so
     return out
 

@@ -28,6 +28,7 @@
 
 #include "../include/gdf.h"
 #include "../include/gdf_p3.h"
+#include "../include/gdf_cy.h"
 
 #include <cmath>
 #include <cstdint>
@@ -1798,6 +1799,7 @@ void default_params(int problem, double* prm) {
 
 #ifndef GDF_ORACLE_NO_P3
 #include "gdf_oracle_p3.inc"
+#include "gdf_oracle_cy.inc"
 #endif
 
 }  // namespace
@@ -2022,6 +2024,47 @@ void orc_p3_basis(void* h, double* out) {
       for (int d = 0; d < NP3; ++d) *q++ = (*T)[g][d];
   for (auto* T : {&o.phiRU, &o.phiLU, &o.phiRD, &o.phiLD, &o.mm})
     for (int d = 0; d < NP3; ++d) *q++ = (*T)[d];
+}
+
+// ------------------------------------------ the cylindrical variant (cy) --
+void* orc_cy_create(const GdfCyConfig* cfg) {
+  if (!cfg) return nullptr;
+  OracleCy* o = new OracleCy();
+  if (!o->setup(*cfg)) { delete o; return nullptr; }
+  return o;
+}
+void orc_cy_destroy(void* h) { delete static_cast<OracleCy*>(h); }
+int orc_cy_init_data(void* h, int problem, double* uh, double* br, double* bz) {
+  static_cast<OracleCy*>(h)->init_data(problem, uh, br, bz);
+  return 0;
+}
+int orc_cy_set_bc(void* h, double* uh) {
+  static_cast<OracleCy*>(h)->set_bc(uh);
+  return 0;
+}
+int orc_cy_lh(void* h, double* uh, double t_rk, double* du, double* dbr, double* dbz) {
+  static_cast<OracleCy*>(h)->lh(uh, t_rk, du, dbr, dbz);
+  return 0;
+}
+int orc_cy_limit(void* h, double* uh, double* br, double* bz, int32_t* flags) {
+  static_cast<OracleCy*>(h)->limit(uh, br, bz, flags);
+  return 0;
+}
+int orc_cy_dt(void* h, const double* uh, double* dt) {
+  *dt = static_cast<OracleCy*>(h)->calc_dt(uh);
+  return 0;
+}
+int orc_cy_step(void* h, double* uh, double* br, double* bz, double* t, double tend, double* dt) {
+  static_cast<OracleCy*>(h)->step(uh, br, bz, t, tend, dt);
+  return 0;
+}
+int orc_cy_diagnostics(void* h, const double* uh, double* umax, double* totaldiv, double* pmin) {
+  static_cast<OracleCy*>(h)->diagnostics(uh, umax, totaldiv, pmin);
+  return 0;
+}
+int orc_cy_l2_error(void* h, int problem, const double* uh, double t, double* l2) {
+  static_cast<OracleCy*>(h)->l2_error(problem, uh, t, l2);
+  return 0;
 }
 #endif
 

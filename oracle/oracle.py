@@ -291,3 +291,93 @@ class OracleP3:
         for k in ("phiRU", "phiLU", "phiRD", "phiLD", "mm"):
             res[k] = out[o:o + 15].copy(); o += 15
         return res
+
+
+# ----------------------------------------------- the cylindrical variant --
+from gdf.cy import GdfCyConfig, cy_new_state  # noqa: E402
+
+
+def _declare_cy(L):
+    if getattr(L, "_cy_declared", False):
+        return L
+    vp, dp, ip = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int32)
+    L.orc_cy_create.restype = vp
+    L.orc_cy_create.argtypes = [C.POINTER(GdfCyConfig)]
+    L.orc_cy_destroy.argtypes = [vp]
+    L.orc_cy_init_data.argtypes = [vp, C.c_int, dp, dp, dp]
+    L.orc_cy_set_bc.argtypes = [vp, dp]
+    L.orc_cy_lh.argtypes = [vp, dp, C.c_double, dp, dp, dp]
+    L.orc_cy_limit.argtypes = [vp, dp, dp, dp, ip]
+    L.orc_cy_dt.argtypes = [vp, dp, dp]
+    L.orc_cy_step.argtypes = [vp, dp, dp, dp, dp, C.c_double, dp]
+    L.orc_cy_diagnostics.argtypes = [vp, dp, dp, dp, dp]
+    L.orc_cy_l2_error.argtypes = [vp, C.c_int, dp, C.c_double, dp]
+    L._cy_declared = True
+    return L
+
+
+class OracleCy:
+    """CPU restatement of MHD_GDF_cy3D_0421/ (Lh, LhEz, TVB_Limiter_P2,
+    div_free_Balsara, set_bc, calculate_dt, RK3, the diagnostics)."""
+
+    def __init__(self, cfg: GdfCyConfig):
+        self.cfg = cfg.copy()
+        self.nr, self.nz, self.lphi = cfg.nr, cfg.nz, cfg.lphi
+        self.L = _declare_cy(lib())
+        self.h = self.L.orc_cy_create(C.byref(self.cfg))
+        if not self.h:
+            raise ValueError("bad oracle configuration")
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h and getattr(self, "L", None) is not None:
+            self.L.orc_cy_destroy(h)
+            self.h = None
+
+    def state(self):
+        return cy_new_state(self.nr, self.nz, self.lphi)
+
+    def init_data(self, problem: int):
+        uh, br, bz = self.state()
+        self.L.orc_cy_init_data(self.h, problem, dptr(uh), dptr(br), dptr(bz))
+        return uh, br, bz
+
+    def set_bc(self, uh):
+        self.L.orc_cy_set_bc(self.h, dptr(uh))
+
+    def lh(self, uh, t_rk: float = 0.0):
+        """Lh then LhEz (set_bc applied to uh in place): du, dbr, dbz."""
+        _, br, bz = self.state()
+        du, dbr, dbz = np.zeros_like(uh), np.zeros_like(br), np.zeros_like(bz)
+        self.L.orc_cy_lh(self.h, dptr(uh), t_rk, dptr(du), dptr(dbr), dptr(dbz))
+        return du, dbr, dbz
+
+    def limit(self, uh, br, bz):
+        """TVB_Limiter_P2 then div_free_Balsara in place; per cell plane
+        (NPH, Nz, Nr) the changed variables (bits 0-7)."""
+        f = np.zeros((2 * self.lphi, self.nz, self.nr), np.int32)
+        self.L.orc_cy_limit(self.h, dptr(uh), dptr(br), dptr(bz), iptr(f))
+        return f
+
+    def dt(self, uh) -> float:
+        d = C.c_double()
+        self.L.orc_cy_dt(self.h, dptr(uh), C.byref(d))
+        return d.value
+
+    def step(self, uh, br, bz, t: float, tend: float):
+        tt = C.c_double(t)
+        dt = C.c_double()
+        self.L.orc_cy_step(self.h, dptr(uh), dptr(br), dptr(bz), C.byref(tt), tend, C.byref(dt))
+        return tt.value, dt.value
+
+    def diagnostics(self, uh):
+        a, b, p = C.c_double(), C.c_double(), C.c_double()
+        self.L.orc_cy_diagnostics(self.h, dptr(uh), C.byref(a), C.byref(b), C.byref(p))
+        return a.value, b.value, p.value
+
+    def l2_error(self, problem: int, uh, t: float) -> np.ndarray:
+        """calculate_L2_error.f90 against the problem's data translated by
+        (t, t): the exact solution of the manufactured problem init1.txt."""
+        out = np.zeros(8)
+        self.L.orc_cy_l2_error(self.h, problem, dptr(uh), t, dptr(out))
+        return out
