@@ -548,7 +548,9 @@ def run_quick(args):
                                HLLD, learned gate) in the persistent kernels
     --workload mlp-train       one epoch of indicator training on 65536
                                synthetic samples (batch 2048)
-    --workload p3-cloud        the k = 3 variant's cloud shock, 2n x n cells"""
+    --workload p3-cloud        the k = 3 variant's cloud shock, 2n x n cells
+    --workload cy-ot           the cylindrical variant's Orszag-Tang vortex,
+                               n x n cells x 2 phi planes"""
     import gdf
     gdf.set_device(dist_env()[2])
     w, n = args.workload, args.n
@@ -570,6 +572,19 @@ def run_quick(args):
         _, k, ms = s.advance_timed(tend if w != "rotor" else 1e9, args.steps)
         print(json.dumps({"quick": True, "workload": w, "n": n, "steps": k, "ms_per_step": ms / max(k, 1),
                           "value": n * n * k / (ms / 1e3)}))
+        s.close()
+        return 0
+    if w == "cy-ot":
+        from gdf import cy
+        cfg, tend = cy.cy_problem_config(cy.CY_ORSZAG_TANG, n, n, 1)
+        s = cy.CySolver(cfg, exact=not args.fma)
+        s.upload(*cy.cy_init_data(cfg, cy.CY_ORSZAG_TANG))
+        s.prepare()
+        if args.warmup:
+            s.advance_timed(tend, args.warmup)
+        _, k, ms = s.advance_timed(tend, args.steps)
+        print(json.dumps({"quick": True, "workload": w, "n": [n, n, 2], "steps": k, "ms_per_step": ms / max(k, 1),
+                          "value": 2 * n * n * k / (ms / 1e3)}))
         s.close()
         return 0
     if w == "p3-cloud":
@@ -793,7 +808,7 @@ def main():
     ap.add_argument("--fma", action="store_true", help="with --quick: run the FMA build")
     ap.add_argument("--n", type=int, default=512, help="with --quick: cells per side")
     ap.add_argument("--workload", default="blast",
-                    choices=["blast", "blast-plain", "rotor", "ensemble-small", "mlp-train", "p3-cloud"],
+                    choices=["blast", "blast-plain", "rotor", "ensemble-small", "mlp-train", "p3-cloud", "cy-ot"],
                     help="with --quick: what to run")
     args = ap.parse_args()
     if args.quick:

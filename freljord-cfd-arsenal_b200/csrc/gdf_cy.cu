@@ -129,36 +129,35 @@ __device__ double S6f(double r, double z, double phi, double t) { return -(0.5 *
 __device__ double S7f(double r, double phi, double t) { return 0.5 * sin(r - t) * cos(phi) / r; }
 
 // The Fourier derivative in phi at one point (Lh.f90:100-122): v holds this
-// lane's plane value, the nph planes of the point sit on adjacent lanes.
+// lane's plane value, the 2*LP planes of the point sit on adjacent lanes.
 // Returns acc + sum_d (Fzzsin(d) sink(kk,d) + Fzzcos(d) cosk(kk,d)) term by
-// term (minus: acc - ... - ...). Every lane of the warp must call it.
+// term (minus: acc - ... - ...). Every lane of the warp must call it. LP is
+// Lphi, a template parameter so the sums unroll to straight-line code.
+template <int LP>
 __device__ __forceinline__ double fourier(const KC& K, double v, int kk, double acc, bool minus) {
-  const int base = (threadIdx.x & 31) & ~(K.nph - 1);
-  double fs[LMAX], fc[LMAX];
+  constexpr int NPH = 2 * LP;
+  const int base = (threadIdx.x & 31) & ~(NPH - 1);
+  double fs[LP], fc[LP];
 #pragma unroll
-  for (int d = 0; d < LMAX; ++d) { fs[d] = 0.0; fc[d] = 0.0; }
+  for (int d = 0; d < LP; ++d) { fs[d] = 0.0; fc[d] = 0.0; }
 #pragma unroll
-  for (int q = 0; q < PMAX; ++q) {
-    if (q < K.nph) {
-      const double f = __shfl_sync(0xffffffffu, v, base + q);
+  for (int q = 0; q < NPH; ++q) {
+    const double f = __shfl_sync(0xffffffffu, v, base + q);
 #pragma unroll
-      for (int d = 0; d < LMAX; ++d)
-        if (d < K.lphi) {
-          fs[d] = fs[d] + K.sink[d][q] * f;
-          fc[d] = fc[d] + K.cosk[d][q] * f;
-        }
+    for (int d = 0; d < LP; ++d) {
+      fs[d] = fs[d] + K.sink[d][q] * f;
+      fc[d] = fc[d] + K.cosk[d][q] * f;
     }
   }
 #pragma unroll
-  for (int d = 0; d < LMAX; ++d)
-    if (d < K.lphi) {
-      const double s = fs[d] / K.lphi, c = fc[d] / K.lphi;
-      const double fzs = -((double)(d + 1) * c), fzc = (double)(d + 1) * s;
-      if (minus)
-        acc = acc - fzs * K.sink[d][kk] - fzc * K.cosk[d][kk];
-      else
-        acc = acc + fzs * K.sink[d][kk] + fzc * K.cosk[d][kk];
-    }
+  for (int d = 0; d < LP; ++d) {
+    const double sd = fs[d] / LP, cd = fc[d] / LP;
+    const double fzs = -((double)(d + 1) * cd), fzc = (double)(d + 1) * sd;
+    if (minus)
+      acc = acc - fzs * K.sink[d][kk] - fzc * K.cosk[d][kk];
+    else
+      acc = acc + fzs * K.sink[d][kk] + fzc * K.cosk[d][kk];
+  }
   return acc;
 }
 
@@ -297,7 +296,7 @@ __global__ void __launch_bounds__(128) k_cy_set_bc(const __grid_constant__ KC K,
 // B traces, the 1-D flux of flux_type (Lh.f90:300-367), the LF edge fields
 // (LhEz.f90:5-34), and their d/dphi over the planes (LhEz.f90:63-127).
 // Output per point (index kk + nph*(g + 5*face)): F[0..6], E, E', dE/dphi.
-template <int DIR>
+template <int DIR, int LP>
 __global__ void __launch_bounds__(128) k_cy_face(const __grid_constant__ KC K, const double* __restrict__ U,
                                                  double* __restrict__ FH, const ScalC* __restrict__ sc) {
   if (sc && !sc->active) return;
@@ -382,7 +381,7 @@ __global__ void __launch_bounds__(128) k_cy_face(const __grid_constant__ KC K, c
     FH[npts * 7 + q] = E1;
     FH[npts * 8 + q] = Ez;
   }
-  const double dE = fourier(K, Ez, kk, 0.0, DIR == 1);
+  const double dE = fourier<LP>(K, Ez, kk, 0.0, DIR == 1);
   if (valid) FH[npts * 9 + q] = dE;
 }
 
@@ -443,7 +442,7 @@ __device__ __forceinline__ double combine(int KIND, double u, double du, double 
   return (1.0 / 3.0) * U0[o] + (2.0 / 3.0) * v;
 }
 
-template <int KIND>
+template <int KIND, int LP>
 __global__ void __launch_bounds__(128) k_cy_cell(const __grid_constant__ KC K, double* __restrict__ U,
                                                  double* __restrict__ X, double* __restrict__ U0,
                                                  double* __restrict__ T, const double* __restrict__ FXH,
@@ -510,7 +509,7 @@ __global__ void __launch_bounds__(128) k_cy_cell(const __grid_constant__ KC K, d
         else if (n == 3) R = -Fx[3] - Fx[3];
         else if (n == 4) R = 0.0 - Fx[4];
         else R = 0.0;
-        if (n < 7) R = fourier(K, Fz[n], kk, R, true);
+        if (n < 7) R = fourier<LP>(K, Fz[n], kk, R, true);
         R = R / rad + C[n];
         const double* PX = K.B.phixG[a][b];
         const double* PY = K.B.phiyG[a][b];
@@ -838,6 +837,7 @@ __global__ void __launch_bounds__(128) k_cy_faceb(const __grid_constant__ KC K, 
 
 // div_free_Balsara.f90:13-147: r*B of every interior cell plane from its
 // four faces and the projection of d(Bphi)/dphi
+template <int LP>
 __global__ void __launch_bounds__(128) k_cy_divfree(const __grid_constant__ KC K, double* __restrict__ U,
                                                     const double* __restrict__ BR, const double* __restrict__ BZ,
                                                     const ScalC* __restrict__ sc) {
@@ -863,7 +863,7 @@ __global__ void __launch_bounds__(128) k_cy_divfree(const __grid_constant__ KC K
       double s = 0.0;
 #pragma unroll
       for (int d = 0; d < NQC; ++d) s = s + m8[d] * G[d];
-      const double dv = fourier(K, s, kk, 0.0, false);
+      const double dv = fourier<LP>(K, s, kk, 0.0, false);
       const double wab = 0.25 * K.B.w[a] * K.B.w[b];
 #pragma unroll
       for (int d = 0; d < NQC; ++d) bpp[d] = bpp[d] + wab * dv * G[d] / K.B.mm[d];
@@ -1001,6 +1001,7 @@ __global__ void __launch_bounds__(DT_BS) k_cy_dt_final(const __grid_constant__ K
 // pressure (calculate_pmin.f90, with the r*B slots as the reference passes
 // them) and, on the plane-0 lane, the cell's sum over (i1, j1, kk) of
 // w w |div B|^2 (calculate_totaldiv.f90:14-68)
+template <int LP>
 __global__ void __launch_bounds__(128) k_cy_diag(const __grid_constant__ KC K, const double* __restrict__ U,
                                                  double* __restrict__ out) {
   const long long q = gtid();
@@ -1023,15 +1024,15 @@ __global__ void __launch_bounds__(128) k_cy_diag(const __grid_constant__ KC K, c
         dv = dv + sv(5, d) * K.B.phixG[a][b][d] + sv(6, d) * K.B.phiyG[a][b][d];
         g8 = g8 + sv(7, d) * K.B.phiG[a][b][d];
       }
-      const double ph = fourier(K, g8, kk, 0.0, false);
+      const double ph = fourier<LP>(K, g8, kk, 0.0, false);
       const double v = (dv + ph) / (rc + K.hr1 * K.B.lam[a]);
       const double term = K.B.w[a] * K.B.w[b] * sq(v);
-      const int base = (threadIdx.x & 31) & ~(K.nph - 1);
-      for (int p = 0; p < PMAX; ++p)
-        if (p < K.nph) {
-          const double tp = __shfl_sync(0xffffffffu, term, base + p);
-          td = td + tp;
-        }
+      const int base = (threadIdx.x & 31) & ~(2 * LP - 1);
+#pragma unroll
+      for (int p = 0; p < 2 * LP; ++p) {
+        const double tp = __shfl_sync(0xffffffffu, term, base + p);
+        td = td + tp;
+      }
       for (int s = 0; s < 2; ++s) {
         double V[NE];
         for (int n = 0; n < NE; ++n) {
@@ -1227,11 +1228,12 @@ int launch_set_bc(GdfCyHandle* h, const ScalC* sc) {
 }
 
 // set_bc, then Lh + LhEz of U fused with the stage's combination (kind)
-int launch_lh(GdfCyHandle* h, int kind, const ScalC* sc) {
+template <int LP>
+int launch_lh_lp(GdfCyHandle* h, int kind, const ScalC* sc) {
   const KC& K = h->K;
   int rc = launch_set_bc(h, sc);
-  if (!rc) rc = run(h, [&] { k_cy_face<0><<<nblk(K.nxf * NG, 128), 128, 0, h->st>>>(K, h->U, h->FXH, sc); });
-  if (!rc) rc = run(h, [&] { k_cy_face<1><<<nblk(K.nyf * NG, 128), 128, 0, h->st>>>(K, h->U, h->FYH, sc); });
+  if (!rc) rc = run(h, [&] { k_cy_face<0, LP><<<nblk(K.nxf * NG, 128), 128, 0, h->st>>>(K, h->U, h->FXH, sc); });
+  if (!rc) rc = run(h, [&] { k_cy_face<1, LP><<<nblk(K.nyf * NG, 128), 128, 0, h->st>>>(K, h->U, h->FYH, sc); });
   if (!rc) rc = run(h, [&] { k_cy_vertex<<<nblk(K.nvx, 128), 128, 0, h->st>>>(K, h->U, h->EzV, sc); });
   if (rc) return rc;
   const unsigned nc = nblk((long long)K.nx * K.ny * K.nph, 128), nf = nblk(K.nxf + K.nyf, 128);
@@ -1239,27 +1241,36 @@ int launch_lh(GdfCyHandle* h, int kind, const ScalC* sc) {
   return run(h, [&] {
     switch (kind) {
       case KIND_LH:
-        k_cy_cell<KIND_LH><<<nc, 128, 0, h->st>>>(K, h->U, h->X, h->U0, h->T, h->FXH, h->FYH, sc);
+        k_cy_cell<KIND_LH, LP><<<nc, 128, 0, h->st>>>(K, h->U, h->X, h->U0, h->T, h->FXH, h->FYH, sc);
         k_cy_bface<KIND_LH><<<nf, 128, 0, h->st>>>(K, h->FXH, h->FYH, h->EzV, h->BR, h->BRX, h->BR0, h->BZ, h->BZX,
                                                     h->BZ0, sc);
         break;
       case KIND_S1:
-        k_cy_cell<KIND_S1><<<nc, 128, 0, h->st>>>(K, h->U, h->X, h->U0, h->T, h->FXH, h->FYH, sc);
+        k_cy_cell<KIND_S1, LP><<<nc, 128, 0, h->st>>>(K, h->U, h->X, h->U0, h->T, h->FXH, h->FYH, sc);
         k_cy_bface<KIND_S1><<<nf, 128, 0, h->st>>>(K, h->FXH, h->FYH, h->EzV, h->BR, h->BRX, h->BR0, h->BZ, h->BZX,
                                                     h->BZ0, sc);
         break;
       case KIND_S2:
-        k_cy_cell<KIND_S2><<<nc, 128, 0, h->st>>>(K, h->U, h->X, h->U0, h->T, h->FXH, h->FYH, sc);
+        k_cy_cell<KIND_S2, LP><<<nc, 128, 0, h->st>>>(K, h->U, h->X, h->U0, h->T, h->FXH, h->FYH, sc);
         k_cy_bface<KIND_S2><<<nf, 128, 0, h->st>>>(K, h->FXH, h->FYH, h->EzV, h->BR, h->BRX, h->BR0, h->BZ, h->BZX,
                                                     h->BZ0, sc);
         break;
       default:
-        k_cy_cell<KIND_S3><<<nc, 128, 0, h->st>>>(K, h->U, h->X, h->U0, h->T, h->FXH, h->FYH, sc);
+        k_cy_cell<KIND_S3, LP><<<nc, 128, 0, h->st>>>(K, h->U, h->X, h->U0, h->T, h->FXH, h->FYH, sc);
         k_cy_bface<KIND_S3><<<nf, 128, 0, h->st>>>(K, h->FXH, h->FYH, h->EzV, h->BR, h->BRX, h->BR0, h->BZ, h->BZX,
                                                     h->BZ0, sc);
         break;
     }
   });
+}
+
+int launch_lh(GdfCyHandle* h, int kind, const ScalC* sc) {
+  switch (h->K.lphi) {
+    case 1: return launch_lh_lp<1>(h, kind, sc);
+    case 2: return launch_lh_lp<2>(h, kind, sc);
+    case 4: return launch_lh_lp<4>(h, kind, sc);
+    default: return launch_lh_lp<8>(h, kind, sc);
+  }
 }
 
 // TVB_Limiter_P2 + div_free_Balsara of (U, BR, BZ) in place
@@ -1271,7 +1282,16 @@ int launch_limit(GdfCyHandle* h, const ScalC* sc, int32_t* flags) {
   if (!rc) rc = run(h, [&] { k_cy_tvb<<<nblk(ncell, 64), 64, 0, h->st>>>(K, h->U, h->BP, flags, sc); });
   if (!rc) rc = launch_set_bc(h, sc);
   if (!rc) rc = run(h, [&] { k_cy_faceb<<<nblk(K.nxf + K.nyf, 128), 128, 0, h->st>>>(K, h->U, h->BR, h->BZ, sc); });
-  if (!rc) rc = run(h, [&] { k_cy_divfree<<<nblk(ncell, 128), 128, 0, h->st>>>(K, h->U, h->BR, h->BZ, sc); });
+  if (!rc)
+    rc = run(h, [&] {
+      const unsigned nb = nblk(ncell, 128);
+      switch (K.lphi) {
+        case 1: k_cy_divfree<1><<<nb, 128, 0, h->st>>>(K, h->U, h->BR, h->BZ, sc); break;
+        case 2: k_cy_divfree<2><<<nb, 128, 0, h->st>>>(K, h->U, h->BR, h->BZ, sc); break;
+        case 4: k_cy_divfree<4><<<nb, 128, 0, h->st>>>(K, h->U, h->BR, h->BZ, sc); break;
+        default: k_cy_divfree<8><<<nb, 128, 0, h->st>>>(K, h->U, h->BR, h->BZ, sc); break;
+      }
+    });
   return rc;
 }
 
@@ -1619,7 +1639,14 @@ int gdf_cy_diagnostics(GdfCyHandle* h, double* umax, double* totaldiv, double* p
   if (!h->uploaded) return fail(GDF_ERR_STATE, "no state uploaded");
   const KC& K = h->K;
   const long long n = (long long)K.nx * K.ny * K.nph;
-  int rc = run(h, [&] { k_cy_diag<<<nblk(n, 128), 128, 0, h->st>>>(K, h->U, h->diag); });
+  int rc = run(h, [&] {
+    switch (K.lphi) {
+      case 1: k_cy_diag<1><<<nblk(n, 128), 128, 0, h->st>>>(K, h->U, h->diag); break;
+      case 2: k_cy_diag<2><<<nblk(n, 128), 128, 0, h->st>>>(K, h->U, h->diag); break;
+      case 4: k_cy_diag<4><<<nblk(n, 128), 128, 0, h->st>>>(K, h->U, h->diag); break;
+      default: k_cy_diag<8><<<nblk(n, 128), 128, 0, h->st>>>(K, h->U, h->diag); break;
+    }
+  });
   if (rc) return rc;
   std::vector<double> v((size_t)n * 3);
   CKC(cudaMemcpyAsync(v.data(), h->diag, v.size() * sizeof(double), cudaMemcpyDeviceToHost, h->st));
