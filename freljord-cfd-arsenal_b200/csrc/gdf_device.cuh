@@ -257,23 +257,69 @@ __device__ __forceinline__ void vertex_item(const Consts& K, const double* __res
 constexpr int CELL_BS = 64;
 
 // ms: the block's NLIVE * CELL_BS staging array (blockDim.x == CELL_BS).
+// PAIRS: ms holds the live slots in pairs (2L, 2L+1) per thread, 16-byte
+// aligned, and the volume loop reads a pair with one 128-bit load (ms must
+// then be 16-byte aligned). SHFL: the x-face fluxes are loaded once per face:
+// each lane reads its cell's right face and takes its left face, the right
+// face of cell i-1, from the lane below by a warp shuffle (lane 0 reads its
+// own); every lane of the warp must then call with consecutive items, valid
+// or not (valid = false: a lane past the array's end, no work). Both leave
+// every value and the order of every sum as they are.
+template <bool SHFL = false, bool PAIRS = false>
 __device__ __forceinline__ void cell_item(const Consts& K, const double* __restrict__ U, double* __restrict__ U0,
                                           double* __restrict__ UI, const double* __restrict__ Fxh,
                                           const double* __restrict__ Fyh, double* __restrict__ duout,
-                                          const Scal* __restrict__ sc, int stage, long long item, double* ms) {
+                                          const Scal* __restrict__ sc, int stage, long long item, double* ms,
+                                          bool valid = true) {
   const int tid = threadIdx.x;
   const int i = (int)(item % K.nx2);
   const int j = (int)(item / K.nx2);
-  const bool interior = i >= 1 && i <= K.nx && j >= 1 && j <= K.ny;
+  const bool interior = valid && i >= 1 && i <= K.nx && j >= 1 && j <= K.ny;
+  auto msi = [&](int L) { return PAIRS ? ((L >> 1) * CELL_BS + tid) * 2 + (L & 1) : L * CELL_BS + tid; };
   double du[NLIVE];
 #pragma unroll
   for (int k = 0; k < NLIVE; ++k) du[k] = 0.0;
+  // Lh.f90:268-304 for variable n from the fluxes of the cell's four faces
+  auto surface = [&](int n, const double* fr, const double* fl, const double* fu, const double* fd) {
+#pragma unroll
+    for (int d = 0; d < NP; ++d) {
+      if (!live_mode(n, d)) continue;
+      double acc = du[LI(n, d)];
+      // at the middle point (lambda = 0) the face basis of modes 3, 5, 8,
+      // 10 (x faces) and 2, 5, 9, 7 (y faces) vanishes on both sides
+#pragma unroll
+      for (int g = 0; g < NG; ++g) {
+        if (g == 2 && (d == 2 || d == 4 || d == 7 || d == 9)) continue;
+        // modes 1 and 2 of the x-face basis are 1 on the right face and
+        // +-1 on the left (get_basis.f90): x * 1 and x * -1 are exact, so
+        // those products are written out
+        const double t = (GDF_FOLD_UNIT && d == 0) ? fr[g] - fl[g]
+                         : (GDF_FOLD_UNIT && d == 1) ? fr[g] - (-fl[g])
+                                                     : fr[g] * c_basis.phiGR[g][d] - fl[g] * c_basis.phiGL[g][d];
+        acc = acc - K.cxs * c_basis.w[g] * t;
+      }
+#pragma unroll
+      for (int g = 0; g < NG; ++g) {
+        if (g == 2 && (d == 1 || d == 4 || d == 8 || d == 6)) continue;
+        // modes 1 and 3 of the y-face basis: 1 on the upper face, +-1 on
+        // the lower
+        const double t = (GDF_FOLD_UNIT && d == 0) ? fu[g] - fd[g]
+                         : (GDF_FOLD_UNIT && d == 2) ? fu[g] - (-fd[g])
+                                                     : fu[g] * c_basis.phiGU[g][d] - fd[g] * c_basis.phiGD[g][d];
+        acc = acc - K.cys * c_basis.w[g] * t;
+      }
+      // mm(1) = 1 (get_basis.f90): x / 1 == x
+      du[LI(n, d)] = (GDF_FOLD_UNIT && d == 0) ? acc
+                     : (n == 3 || n == 7)     ? dv(acc, c_basis.mm[d])
+                                              : acc / c_basis.mm[d];
+    }
+  };
   if (interior) {
 #pragma unroll
     for (int n = 0; n < NE; ++n)
 #pragma unroll
       for (int d = 0; d < NP; ++d)
-        if (live_mode(n, d)) ms[LI(n, d) * CELL_BS + tid] = U[item + K.plane * (d + 10 * n)];
+        if (live_mode(n, d)) ms[msi(LI(n, d))] = U[item + K.plane * (d + 10 * n)];
     if (GDF_CELL_PREFETCH) {
       // the surface term reads the fluxes of the cell's four faces after the
       // volume loop: ask for them in L2 now, so the loads that follow the
@@ -296,12 +342,24 @@ __device__ __forceinline__ void cell_item(const Consts& K, const double* __restr
 #pragma unroll
         for (int n = 0; n < NE; ++n) {
           double acc = 0.0;
+          double mv[8];
+          if (PAIRS) {
+            const int nl = (n == 5 || n == 6) ? 8 : 6;
+#pragma unroll
+            for (int k = 0; k < 8; k += 2)
+              if (k < nl) {
+                const double2 q = reinterpret_cast<const double2*>(ms)[((LI(n, 0) + k) >> 1) * CELL_BS + tid];
+                mv[k] = q.x;
+                mv[k + 1] = q.y;
+              }
+          }
 #pragma unroll
           for (int d = 0; d < NP; ++d) {
             if (!live_mode(n, d)) continue;
+            const double m = PAIRS ? mv[LI(n, d) - LI(n, 0)] : ms[LI(n, d) * CELL_BS + tid];
             // mode 1 of the volume basis is 1 at every point: m * 1 == m
-            if (GDF_FOLD_UNIT && d == 0) acc = acc + ms[LI(n, d) * CELL_BS + tid];
-            else acc = acc + ms[LI(n, d) * CELL_BS + tid] * c_basis.phiG[a][b][d];
+            if (GDF_FOLD_UNIT && d == 0) acc = acc + m;
+            else acc = acc + m * c_basis.phiG[a][b][d];
           }
           v[n] = acc;
         }
@@ -350,53 +408,50 @@ __device__ __forceinline__ void cell_item(const Consts& K, const double* __restr
           }
       }
     }
-    // surface terms in the reference order (x faces, then y faces), mass
-    const long long ox = (i - 1) + 1 + (long long)(K.nx + 1) * (j - 1);  // Fxhat(i,j)
-    const long long oy = (i - 1) + (long long)K.nx * j;                  // Fyhat(i,j)
+    if (!SHFL) {
+      // surface terms in the reference order (x faces, then y faces), mass
+      const long long ox = (i - 1) + 1 + (long long)(K.nx + 1) * (j - 1);  // Fxhat(i,j)
+      const long long oy = (i - 1) + (long long)K.nx * j;                  // Fyhat(i,j)
+#pragma unroll
+      for (int n = 0; n < NE; ++n) {
+        double fr[NG], fl[NG], fu[NG], fd[NG];
+#pragma unroll
+        for (int g = 0; g < NG; ++g) {
+          fr[g] = Fxh[(n * NG + g) * K.fxplane + ox];
+          fl[g] = Fxh[(n * NG + g) * K.fxplane + ox - 1];
+          fu[g] = Fyh[(n * NG + g) * K.fyplane + oy];
+          fd[g] = Fyh[(n * NG + g) * K.fyplane + oy - K.nx];
+        }
+        surface(n, fr, fl, fu, fd);
+      }
+    }
+  }
+  if (SHFL) {
+    // the right x face of every cell of rows 1..ny with i <= nx (ghost
+    // column 0 included: its right face is the left face of cell 1)
+    const bool has_r = valid && j >= 1 && j <= K.ny && i <= K.nx;
+    const long long ox = i + (long long)(K.nx + 1) * (j - 1);  // Fxhat(i,j)
+    const long long oy = (i - 1) + (long long)K.nx * j;        // Fyhat(i,j)
+    const bool own_l = (threadIdx.x & 31) == 0;
 #pragma unroll
     for (int n = 0; n < NE; ++n) {
       double fr[NG], fl[NG], fu[NG], fd[NG];
 #pragma unroll
-      for (int g = 0; g < NG; ++g) {
-        fr[g] = Fxh[(n * NG + g) * K.fxplane + ox];
-        fl[g] = Fxh[(n * NG + g) * K.fxplane + ox - 1];
-        fu[g] = Fyh[(n * NG + g) * K.fyplane + oy];
-        fd[g] = Fyh[(n * NG + g) * K.fyplane + oy - K.nx];
-      }
+      for (int g = 0; g < NG; ++g) fr[g] = has_r ? Fxh[(n * NG + g) * K.fxplane + ox] : 0.0;
 #pragma unroll
-      for (int d = 0; d < NP; ++d) {
-        if (!live_mode(n, d)) continue;
-        double acc = du[LI(n, d)];
-        // at the middle point (lambda = 0) the face basis of modes 3, 5, 8,
-        // 10 (x faces) and 2, 5, 9, 7 (y faces) vanishes on both sides
+      for (int g = 0; g < NG; ++g) fl[g] = __shfl_up_sync(0xffffffffu, fr[g], 1);
+      if (interior) {
 #pragma unroll
         for (int g = 0; g < NG; ++g) {
-          if (g == 2 && (d == 2 || d == 4 || d == 7 || d == 9)) continue;
-          // modes 1 and 2 of the x-face basis are 1 on the right face and
-          // +-1 on the left (get_basis.f90): x * 1 and x * -1 are exact, so
-          // those products are written out
-          const double t = (GDF_FOLD_UNIT && d == 0) ? fr[g] - fl[g]
-                           : (GDF_FOLD_UNIT && d == 1) ? fr[g] - (-fl[g])
-                                                       : fr[g] * c_basis.phiGR[g][d] - fl[g] * c_basis.phiGL[g][d];
-          acc = acc - K.cxs * c_basis.w[g] * t;
+          if (own_l) fl[g] = Fxh[(n * NG + g) * K.fxplane + ox - 1];
+          fu[g] = Fyh[(n * NG + g) * K.fyplane + oy];
+          fd[g] = Fyh[(n * NG + g) * K.fyplane + oy - K.nx];
         }
-#pragma unroll
-        for (int g = 0; g < NG; ++g) {
-          if (g == 2 && (d == 1 || d == 4 || d == 8 || d == 6)) continue;
-          // modes 1 and 3 of the y-face basis: 1 on the upper face, +-1 on
-          // the lower
-          const double t = (GDF_FOLD_UNIT && d == 0) ? fu[g] - fd[g]
-                           : (GDF_FOLD_UNIT && d == 2) ? fu[g] - (-fd[g])
-                                                       : fu[g] * c_basis.phiGU[g][d] - fd[g] * c_basis.phiGD[g][d];
-          acc = acc - K.cys * c_basis.w[g] * t;
-        }
-        // mm(1) = 1 (get_basis.f90): x / 1 == x
-        du[LI(n, d)] = (GDF_FOLD_UNIT && d == 0) ? acc
-                       : (n == 3 || n == 7)     ? dv(acc, c_basis.mm[d])
-                                                : acc / c_basis.mm[d];
+        surface(n, fr, fl, fu, fd);
       }
     }
   }
+  if (!valid) return;
   if (stage == 0) {
     if (interior) {
 #pragma unroll

@@ -60,6 +60,15 @@
 #ifndef GDF_CELL_MINB
 #define GDF_CELL_MINB 1
 #endif
+// k_cell: x-face fluxes shared between neighbouring lanes by warp shuffles
+// (GDF_CELL_SHFL) and the staged modes read in pairs (GDF_CELL_PAIRS); same
+// values either way
+#ifndef GDF_CELL_SHFL
+#define GDF_CELL_SHFL 0
+#endif
+#ifndef GDF_CELL_PAIRS
+#define GDF_CELL_PAIRS 0
+#endif
 #ifndef GDF_LIMIT_MINB
 #define GDF_LIMIT_MINB 1
 #endif
@@ -116,11 +125,16 @@ __global__ void __launch_bounds__(CELL_BS, GDF_CELL_MINB) k_cell(const __grid_co
                                                   double* __restrict__ U0, double* __restrict__ UI,
                                                   const double* __restrict__ Fxh, const double* __restrict__ Fyh,
                                                   double* __restrict__ duout, const Scal* __restrict__ sc, int stage) {
-  __shared__ double ms[NLIVE * CELL_BS];
+  __shared__ __align__(16) double ms[NLIVE * CELL_BS];
   if (sc && !sc->active) return;
   const long long item = gtid();
+  if (GDF_CELL_SHFL) {
+    // every lane takes part in the x-face shuffles, past the end too
+    cell_item<true, GDF_CELL_PAIRS != 0>(K, U, U0, UI, Fxh, Fyh, duout, sc, stage, item, ms, item < K.plane);
+    return;
+  }
   if (item >= K.plane) return;
-  cell_item(K, U, U0, UI, Fxh, Fyh, duout, sc, stage, item, ms);
+  cell_item<false, GDF_CELL_PAIRS != 0>(K, U, U0, UI, Fxh, Fyh, duout, sc, stage, item, ms);
 }
 
 __global__ void __launch_bounds__(128) k_bface(const __grid_constant__ Consts K, const double* __restrict__ EzRL,
@@ -258,6 +272,34 @@ __global__ void k_divfree(const __grid_constant__ Consts K, double* __restrict__
   const long long item = gtid();
   if (item >= (long long)K.nx * K.ny) return;
   divfree_item(K, D, BX, BY, item);
+}
+
+// The step state in its smallest form (gdf_upload_state/gdf_download_state):
+// modes 1-6 of the six variables a step evolves in the cell (rho, rho u,
+// rho v, rho w, E, Bz) over the interior cells, packed as
+// cells[i + nx*(j + ny*(d + 6*v))]. The cell Bx/By modes are not part of
+// it: div_free_Balsara rebuilds them from the face fields at the end of
+// every stage, and the ghosts are set_bc of the interior.
+__device__ __forceinline__ long long state_slot(const Consts& K, long long item) {
+  const long long ncell = (long long)K.nx * K.ny;
+  const int s = (int)(item / ncell);
+  const long long q = item - s * ncell;
+  const int i = (int)(q % K.nx) + 1, j = (int)(q / K.nx) + 1;
+  const int d = s % 6, v = s / 6;
+  const int n = v < 5 ? v : 7;
+  return i + (long long)K.nx2 * j + K.plane * (d + 10 * n);
+}
+__global__ void k_pack_state(const __grid_constant__ Consts K, const double* __restrict__ U,
+                             double* __restrict__ cells) {
+  const long long item = gtid();
+  if (item >= 36LL * K.nx * K.ny) return;
+  cells[item] = U[state_slot(K, item)];
+}
+__global__ void k_unpack_state(const __grid_constant__ Consts K, const double* __restrict__ cells,
+                               double* __restrict__ U) {
+  const long long item = gtid();
+  if (item >= 36LL * K.nx * K.ny) return;
+  U[state_slot(K, item)] = cells[item];
 }
 
 // calculate_dt.f90:11-25: per-block maxima of |u_n +- c_f| over the cell
@@ -875,6 +917,18 @@ static int ensure_graph(GdfHandle* h) {
   return GDF_OK;
 }
 
+static size_t state_bytes(const GdfConfig& c) { return (size_t)36 * c.nx * c.ny * sizeof(double); }
+
+// A launch outside the step (state transfer): counted, its error reported.
+template <class F>
+static int run_plain(GdfHandle* h, F&& launch) {
+  launch();
+  h->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(GDF_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+  return GDF_OK;
+}
+
 extern "C" {
 
 const char* gdf_last_error(void) { return g_err.c_str(); }
@@ -1008,6 +1062,43 @@ int gdf_download_live(GdfHandle* h, double* uh, double* bx, double* by) {
   if (!h) return fail(GDF_ERR_ARG, "null handle");
   if (!h->uploaded) return fail(GDF_ERR_STATE, "no state uploaded");
   if (uh) CK(copy_live(uh, h->U, h->cfg, h->st, cudaMemcpyDeviceToHost));
+  if (bx) CK(cudaMemcpyAsync(bx, h->BX, bx_bytes(h->cfg), cudaMemcpyDeviceToHost, h->st));
+  if (by) CK(cudaMemcpyAsync(by, h->BY, by_bytes(h->cfg), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return GDF_OK;
+}
+
+int gdf_upload_state(GdfHandle* h, const double* cells, const double* bx, const double* by) {
+  if (!h || !cells || !bx || !by) return fail(GDF_ERR_ARG, "null argument");
+  const Consts& K = h->K;
+  const long long n = 36LL * K.nx * K.ny;
+  CK(cudaMemcpyAsync(h->UT, cells, state_bytes(h->cfg), cudaMemcpyHostToDevice, h->st));
+  CK(cudaMemcpyAsync(h->BX, bx, bx_bytes(h->cfg), cudaMemcpyHostToDevice, h->st));
+  CK(cudaMemcpyAsync(h->BY, by, by_bytes(h->cfg), cudaMemcpyHostToDevice, h->st));
+  int rc = run_plain(h, [&] { k_unpack_state<<<nblk(n, 256), 256, 0, h->st>>>(K, h->UT, h->U); });
+  // the cell B modes from the face fields (div_free_Balsara.f90:13-79), the
+  // ghosts as the end of a stage leaves them (set_bc with the ghost B
+  // modes cleared, div_free_Balsara.f90:11)
+  if (!rc) rc = run_plain(h, [&] { k_divfree<<<nblk((long long)K.nx * K.ny, 128), 128, 0, h->st>>>(K, h->U, h->BX, h->BY, nullptr); });
+  if (!rc) {
+    const long long nb = (2LL * (K.nx + 2) + 2LL * K.ny) * NLIVE;
+    rc = run_plain(h, [&] { k_set_bc<<<nblk(nb, 256), 256, 0, h->st>>>(K, h->U, 1, nullptr); });
+  }
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(h->st));
+  h->uploaded = 1;
+  return GDF_OK;
+}
+
+int gdf_download_state(GdfHandle* h, double* cells, double* bx, double* by) {
+  if (!h) return fail(GDF_ERR_ARG, "null handle");
+  if (!h->uploaded) return fail(GDF_ERR_STATE, "no state uploaded");
+  if (cells) {
+    const long long n = 36LL * h->K.nx * h->K.ny;
+    int rc = run_plain(h, [&] { k_pack_state<<<nblk(n, 256), 256, 0, h->st>>>(h->K, h->U, h->UT); });
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(cells, h->UT, state_bytes(h->cfg), cudaMemcpyDeviceToHost, h->st));
+  }
   if (bx) CK(cudaMemcpyAsync(bx, h->BX, bx_bytes(h->cfg), cudaMemcpyDeviceToHost, h->st));
   if (by) CK(cudaMemcpyAsync(by, h->BY, by_bytes(h->cfg), cudaMemcpyDeviceToHost, h->st));
   CK(cudaStreamSynchronize(h->st));

@@ -55,6 +55,19 @@ module gdf_bind
       type(c_ptr), value :: h
       real(c_double), intent(out) :: uh(*), bx(*), by(*)
     end function
+    ! the step state in its smallest form: cells(Nx, Ny, 6, 6) holds modes
+    ! 1-6 of variables 1-5 and 8 over the interior cells; the device rebuilds
+    ! the cell B modes (div_free_Balsara) and the ghosts (set_bc)
+    integer(c_int) function gdf_upload_state(h, cells, bx, by) bind(c, name="gdf_upload_state")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: h
+      real(c_double), intent(in) :: cells(*), bx(*), by(*)
+    end function
+    integer(c_int) function gdf_download_state(h, cells, bx, by) bind(c, name="gdf_download_state")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: h
+      real(c_double), intent(out) :: cells(*), bx(*), by(*)
+    end function
     ! init_data.f90 on the device, into the handle's state (params may be
     ! c_null_ptr for the problem's defaults)
     integer(c_int) function gdf_init_data_device(h, problem, params) bind(c, name="gdf_init_data_device")

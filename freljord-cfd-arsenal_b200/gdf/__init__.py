@@ -72,6 +72,8 @@ def load(exact: bool = True):
     L.gdf_upload.argtypes = [vp, dp, dp, dp]
     L.gdf_download.argtypes = [vp, dp, dp, dp]
     L.gdf_download_live.argtypes = [vp, dp, dp, dp]
+    L.gdf_upload_state.argtypes = [vp, dp, dp, dp]
+    L.gdf_download_state.argtypes = [vp, dp, dp, dp]
     L.gdf_prepare.argtypes = [vp, ip]
     L.gdf_step.argtypes = [vp, C.c_double, dp, dp, ip]
     L.gdf_advance.argtypes = [vp, C.c_double, i32, dp, ip]
@@ -261,6 +263,25 @@ class Solver:
         live_only: gdf_download_live (dead slot planes of uh not written)."""
         f = self.L.gdf_download_live if live_only else self.L.gdf_download
         _check(self.L, f(self.h, dptr(uh), dptr(bx), dptr(by)))
+
+    def state_shape(self) -> tuple:
+        """numpy shape (v, d, j, i) of the compact step state of
+        gdf_upload_state / gdf_download_state: modes 1-6 of variables
+        1-5 and 8 over the interior cells."""
+        return (6, 6, self.ny, self.nx)
+
+    def upload_state(self, cells, bx, by) -> None:
+        """gdf_upload_state: the compact state; the device rebuilds the cell
+        B modes (div-free reconstruction) and the ghosts (set_bc)."""
+        _check(self.L, self.L.gdf_upload_state(self.h, dptr(cells), dptr(bx), dptr(by)))
+
+    def download_state(self, cells=None, bx=None, by=None):
+        """gdf_download_state into caller arrays (allocated when None)."""
+        if cells is None:
+            cells = np.zeros(self.state_shape())
+            _, bx, by = new_state(self.nx, self.ny)
+        _check(self.L, self.L.gdf_download_state(self.h, dptr(cells), dptr(bx), dptr(by)))
+        return cells, bx, by
 
     def prepare(self):
         f = self._flags()

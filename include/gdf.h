@@ -142,6 +142,25 @@ int gdf_download(GdfHandle *h, double *uh, double *bx, double *by);
  * reference's COMMON block, already holds zeros there). 35% less
  * device-to-host traffic per call. No counterpart in the reference. */
 int gdf_download_live(GdfHandle *h, double *uh, double *bx, double *by);
+/* The state a step needs and produces, in its smallest form (synchronous).
+ * Replaces the transfer of uh(0:Nx+1,0:Ny+1,10,8) plus Bx/By (com.txt:48)
+ * for a host that round-trips the state every step; no counterpart in the
+ * reference. cells holds modes 1-6 of the six variables that evolve in the
+ * cell (reference variables 1-5: rho, rho u, rho v, rho w, E, and 8: Bz)
+ * over the interior cells, cells[i + Nx*(j + Ny*(d + 6*v))] for cell
+ * (i+1, j+1), mode d+1, v = 0..5 for variables 1, 2, 3, 4, 5, 8 (36 Nx Ny
+ * doubles); bx, by are the reference's face arrays. The rest of uh is a
+ * function of these: the cell Bx/By modes are div_free_Balsara of the face
+ * fields (div_free_Balsara.f90:13-79, the last write to them in every
+ * stage), the ghosts are set_bc of the interior with the ghost B modes
+ * cleared (how every step leaves them, div_free_Balsara.f90:11).
+ * gdf_upload_state rebuilds them on the device, so a step after it equals,
+ * value for value, a step of the state gdf_download_state returned; 28%
+ * fewer bytes cross the bus each way than with gdf_upload and
+ * gdf_download_live. A host that needs the full uh rebuilds it with the
+ * reference's own div_free_Balsara and set_bc, or calls gdf_download. */
+int gdf_upload_state(GdfHandle *h, const double *cells, const double *bx, const double *by);
+int gdf_download_state(GdfHandle *h, double *cells, double *bx, double *by);
 
 /* RK3.f90:5-12: t = 0, set_bc, TVB_Limiter_P2, div_free_Balsara on the
  * resident state. flags (may be NULL) receives the troubled-cell word of
