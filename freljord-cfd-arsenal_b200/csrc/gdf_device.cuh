@@ -256,6 +256,13 @@ __device__ __forceinline__ void vertex_item(const Consts& K, const double* __res
 // du = 0, as Lh leaves them). stage 0 writes du instead (gdf_lh).
 constexpr int CELL_BS = 64;
 
+// The residual kernels read their staged modes in pairs, one 128-bit
+// shared-memory load per two modes: blast 2048^2 step 45.6 against 46.5 ms,
+// same values (GDF_CELL_PAIRS=0: one 64-bit load per mode).
+#ifndef GDF_CELL_PAIRS
+#define GDF_CELL_PAIRS 1
+#endif
+
 // ms: the block's NLIVE * CELL_BS staging array (blockDim.x == CELL_BS).
 // PAIRS: ms holds the live slots in pairs (2L, 2L+1) per thread, 16-byte
 // aligned, and the volume loop reads a pair with one 128-bit load (ms must
@@ -1115,13 +1122,15 @@ __device__ __forceinline__ void char_limit_dir(const Consts& K, int dir, double 
 
 // STREAM: lim_tvb through char_limit_dir (one eigenvector matrix live at a
 // time) instead of both matrices at once; same values. GDF_TVB_STREAM=1
-// gives it to the second limiter pass: k_limit_tvb 0.50 against 0.60 ms
-// per launch on the developed rotor 512^2, but the blast 2048^2 step, which
-// never launches that kernel, measured 46.3 against 45.5 ms with it (three
-// A/B pairs, equal hashes; a build of the same source by another route
-// measured the same), so the product keeps it off.
+// (the default) gives it to the second limiter pass: with the paired
+// residual loads, the developed rotor 512^2 (steps 104-303) runs 4.86
+// against 4.94 ms per step (k_limit_tvb 0.48 against 0.51 ms per launch)
+// and the blast 2048^2 step, which never launches that kernel, is unchanged
+// (45.64 against 45.65 ms), two A/B pairs with equal hashes. An earlier
+// build without the paired loads had measured that blast step 46.3 against
+// 45.5 ms with it.
 #ifndef GDF_TVB_STREAM
-#define GDF_TVB_STREAM 0
+#define GDF_TVB_STREAM 1
 #endif
 
 template <bool ROLLED = false, bool STREAM = false>

@@ -102,7 +102,8 @@ __device__ __noinline__ void call_vertex(const Consts& K, const double* U, doubl
 extern __shared__ __align__(16) unsigned char ens_sm[];   // the stage kernel's dynamic shared memory
 __device__ __noinline__ void call_cell(const Consts& K, const double* U, double* U0, double* UI, const double* Fxh,
                                        const double* Fyh, const Scal* sc, int stage, long long item) {
-  cell_item(K, U, U0, UI, Fxh, Fyh, nullptr, sc, stage, item, reinterpret_cast<double*>(ens_sm));
+  cell_item<false, GDF_CELL_PAIRS != 0>(K, U, U0, UI, Fxh, Fyh, nullptr, sc, stage, item,
+                                        reinterpret_cast<double*>(ens_sm));
 }
 __device__ __noinline__ void call_bface(const Consts& K, const double* EzRL, const double* EzUD, const double* EzV,
                                         double* BX, double* BX0, double* BXI, double* BY, double* BY0, double* BYI,
@@ -439,11 +440,13 @@ __global__ void __launch_bounds__(ENS_BS, 8) k_ep_faces(const __grid_constant__ 
 }
 
 __global__ void __launch_bounds__(ENS_BS) k_ep_cell(const __grid_constant__ EnsArgs A, int stage) {
-  __shared__ double ms[NLIVE * ENS_BS];
+  static_assert(ENS_BS == CELL_BS, "cell_item's staging stride is CELL_BS");
+  __shared__ __align__(16) double ms[NLIVE * ENS_BS];
   for_tiles<true>(A, EK_CELL, [&](int, const EnsInst& I, const Consts& K, long long base, int per) {
     for (int k = threadIdx.x; k < per; k += ENS_BS) {
       const long long item = base + k;
-      if (item < K.plane) cell_item(K, I.U, I.U0, I.UI, I.Fxh, I.Fyh, nullptr, I.sc, stage, item, ms);
+      if (item < K.plane)
+        cell_item<false, GDF_CELL_PAIRS != 0>(K, I.U, I.U0, I.UI, I.Fxh, I.Fyh, nullptr, I.sc, stage, item, ms);
     }
   });
 }

@@ -60,14 +60,12 @@
 #ifndef GDF_CELL_MINB
 #define GDF_CELL_MINB 1
 #endif
-// k_cell: x-face fluxes shared between neighbouring lanes by warp shuffles
-// (GDF_CELL_SHFL) and the staged modes read in pairs (GDF_CELL_PAIRS); same
-// values either way
+// k_cell reads its staged modes in pairs (GDF_CELL_PAIRS, in
+// gdf_device.cuh). GDF_CELL_SHFL=1 loads every x-face flux once and passes the left
+// face of a cell from the lane below by a warp shuffle: 12% slower k_cell
+// (246 registers, the surface loads taken out of the interior branch), off.
 #ifndef GDF_CELL_SHFL
 #define GDF_CELL_SHFL 0
-#endif
-#ifndef GDF_CELL_PAIRS
-#define GDF_CELL_PAIRS 0
 #endif
 #ifndef GDF_LIMIT_MINB
 #define GDF_LIMIT_MINB 1

@@ -279,6 +279,7 @@ class Solver:
         """gdf_download_state into caller arrays (allocated when None)."""
         if cells is None:
             cells = np.zeros(self.state_shape())
+        if bx is None or by is None:
             _, bx, by = new_state(self.nx, self.ny)
         _check(self.L, self.L.gdf_download_state(self.h, dptr(cells), dptr(bx), dptr(by)))
         return cells, bx, by
