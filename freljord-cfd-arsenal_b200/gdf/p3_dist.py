@@ -208,7 +208,7 @@ class DistTransport:
         return float(v[0]), float(v[1])
 
 
-# ------------------------------------------------------------ the driver --
+# ------------------------------------------------- decomposed stepping --
 
 class _DeviceArray:
     """A raw device pointer as an object torch.as_tensor can view."""
