@@ -442,11 +442,20 @@ __device__ __forceinline__ double combine(int KIND, double u, double du, double 
   return (1.0 / 3.0) * U0[o] + (2.0 / 3.0) * v;
 }
 
+// k_cy_cell stages the 54 slots of its cell plane in shared memory once and
+// reads them there at each of the 25 Gauss points (GDF_CY_STAGE=0: every
+// point reads them from global memory through L1)
+#ifndef GDF_CY_STAGE
+#define GDF_CY_STAGE 1
+#endif
+constexpr int CY_CELL_BS = GDF_CY_STAGE ? 64 : 128;
+
 template <int KIND, int LP>
-__global__ void __launch_bounds__(128) k_cy_cell(const __grid_constant__ KC K, double* __restrict__ U,
-                                                 double* __restrict__ X, double* __restrict__ U0,
-                                                 double* __restrict__ T, const double* __restrict__ FXH,
-                                                 const double* __restrict__ FYH, const ScalC* __restrict__ sc) {
+__global__ void __launch_bounds__(CY_CELL_BS) k_cy_cell(const __grid_constant__ KC K, double* __restrict__ U,
+                                                        double* __restrict__ X, double* __restrict__ U0,
+                                                        double* __restrict__ T, const double* __restrict__ FXH,
+                                                        const double* __restrict__ FYH, const ScalC* __restrict__ sc) {
+  __shared__ double cms[GDF_CY_STAGE ? NSC * CY_CELL_BS : 1];
   if (KIND != KIND_LH && !sc->active) return;
   const long long q = gtid();
   const long long nitem = (long long)K.nx * K.ny * K.nph;
@@ -463,6 +472,13 @@ __global__ void __launch_bounds__(128) k_cy_cell(const __grid_constant__ KC K, d
   for (int n = 0; n < NE; ++n)
 #pragma unroll
     for (int d = 0; d < NQC; ++d) du[n][d] = 0.0;
+  if (GDF_CY_STAGE) {
+    // each thread stages its own plane's slots (its own column: no barrier);
+    // a thread past the end sees rho = 1 and zeros, as below
+#pragma unroll 6
+    for (int sl = 0; sl < NSC; ++sl)
+      cms[sl * CY_CELL_BS + threadIdx.x] = valid ? ld(U + cp + K.ncp * sl) : (sl == 0 ? 1.0 : 0.0);
+  }
   // volume (Lh.f90:14-146)
 #pragma unroll 1
   for (int a = 0; a < NG; ++a) {
@@ -477,7 +493,9 @@ __global__ void __launch_bounds__(128) k_cy_cell(const __grid_constant__ KC K, d
 #pragma unroll
         for (int d = 0; d < NPC; ++d) {
           const int sl = slotc(n, d);
-          if (sl >= 0) s = s + (valid ? ld(U + cp + K.ncp * sl) : (n == 0 && d == 0 ? 1.0 : 0.0)) * G[d];
+          if (sl >= 0)
+            s = s + (GDF_CY_STAGE ? cms[sl * CY_CELL_BS + threadIdx.x]
+                                  : (valid ? ld(U + cp + K.ncp * sl) : (n == 0 && d == 0 ? 1.0 : 0.0))) * G[d];
         }
         Uv[n] = s;
       }
@@ -1236,27 +1254,27 @@ int launch_lh_lp(GdfCyHandle* h, int kind, const ScalC* sc) {
   if (!rc) rc = run(h, [&] { k_cy_face<1, LP><<<nblk(K.nyf * NG, 128), 128, 0, h->st>>>(K, h->U, h->FYH, sc); });
   if (!rc) rc = run(h, [&] { k_cy_vertex<<<nblk(K.nvx, 128), 128, 0, h->st>>>(K, h->U, h->EzV, sc); });
   if (rc) return rc;
-  const unsigned nc = nblk((long long)K.nx * K.ny * K.nph, 128), nf = nblk(K.nxf + K.nyf, 128);
+  const unsigned nc = nblk((long long)K.nx * K.ny * K.nph, CY_CELL_BS), nf = nblk(K.nxf + K.nyf, 128);
   h->launches++;  // the pair below is two launches
   return run(h, [&] {
     switch (kind) {
       case KIND_LH:
-        k_cy_cell<KIND_LH, LP><<<nc, 128, 0, h->st>>>(K, h->U, h->X, h->U0, h->T, h->FXH, h->FYH, sc);
+        k_cy_cell<KIND_LH, LP><<<nc, CY_CELL_BS, 0, h->st>>>(K, h->U, h->X, h->U0, h->T, h->FXH, h->FYH, sc);
         k_cy_bface<KIND_LH><<<nf, 128, 0, h->st>>>(K, h->FXH, h->FYH, h->EzV, h->BR, h->BRX, h->BR0, h->BZ, h->BZX,
                                                     h->BZ0, sc);
         break;
       case KIND_S1:
-        k_cy_cell<KIND_S1, LP><<<nc, 128, 0, h->st>>>(K, h->U, h->X, h->U0, h->T, h->FXH, h->FYH, sc);
+        k_cy_cell<KIND_S1, LP><<<nc, CY_CELL_BS, 0, h->st>>>(K, h->U, h->X, h->U0, h->T, h->FXH, h->FYH, sc);
         k_cy_bface<KIND_S1><<<nf, 128, 0, h->st>>>(K, h->FXH, h->FYH, h->EzV, h->BR, h->BRX, h->BR0, h->BZ, h->BZX,
                                                     h->BZ0, sc);
         break;
       case KIND_S2:
-        k_cy_cell<KIND_S2, LP><<<nc, 128, 0, h->st>>>(K, h->U, h->X, h->U0, h->T, h->FXH, h->FYH, sc);
+        k_cy_cell<KIND_S2, LP><<<nc, CY_CELL_BS, 0, h->st>>>(K, h->U, h->X, h->U0, h->T, h->FXH, h->FYH, sc);
         k_cy_bface<KIND_S2><<<nf, 128, 0, h->st>>>(K, h->FXH, h->FYH, h->EzV, h->BR, h->BRX, h->BR0, h->BZ, h->BZX,
                                                     h->BZ0, sc);
         break;
       default:
-        k_cy_cell<KIND_S3, LP><<<nc, 128, 0, h->st>>>(K, h->U, h->X, h->U0, h->T, h->FXH, h->FYH, sc);
+        k_cy_cell<KIND_S3, LP><<<nc, CY_CELL_BS, 0, h->st>>>(K, h->U, h->X, h->U0, h->T, h->FXH, h->FYH, sc);
         k_cy_bface<KIND_S3><<<nf, 128, 0, h->st>>>(K, h->FXH, h->FYH, h->EzV, h->BR, h->BRX, h->BR0, h->BZ, h->BZX,
                                                     h->BZ0, sc);
         break;
