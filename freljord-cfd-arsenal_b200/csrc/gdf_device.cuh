@@ -96,9 +96,14 @@ __host__ __device__ __forceinline__ long long face_items(const Consts& K) {
 // mL(n, d) (the cell on the low side) and mR(n, d) (the high side); o is the
 // face's offset in its plane. The arithmetic is that of Lh.f90:72-265 and
 // LhEz.f90:6-31 whichever memory the modes come from.
-template <int DIR, class ML, class MR>
+// SMB: the face basis is read from sb, a copy in shared memory of the low
+// cell's table (phiGR / phiGU) followed by the high cell's (phiGL / phiGD),
+// [2][NG][NP], for lanes whose points g differ (the constant cache would
+// serialise their addresses).
+template <int DIR, bool SMB = false, class ML, class MR>
 __device__ __forceinline__ void face_point(const Consts& K, ML mL, MR mR, int g, double* __restrict__ Fh_out,
-                                           double* __restrict__ Ez_out, long long o) {
+                                           double* __restrict__ Ez_out, long long o,
+                                           const double* __restrict__ sb = nullptr) {
   double uL[NE], uR[NE];
 #pragma unroll
   for (int n = 0; n < NE; ++n) {
@@ -106,8 +111,8 @@ __device__ __forceinline__ void face_point(const Consts& K, ML mL, MR mR, int g,
 #pragma unroll
     for (int d = 0; d < NP; ++d) {
       if (!live_mode(n, d)) continue;
-      const double pl = DIR == 0 ? c_basis.phiGR[g][d] : c_basis.phiGU[g][d];
-      const double pr = DIR == 0 ? c_basis.phiGL[g][d] : c_basis.phiGD[g][d];
+      const double pl = SMB ? sb[g * NP + d] : DIR == 0 ? c_basis.phiGR[g][d] : c_basis.phiGU[g][d];
+      const double pr = SMB ? sb[(NG + g) * NP + d] : DIR == 0 ? c_basis.phiGL[g][d] : c_basis.phiGD[g][d];
       // the face basis is 1 for mode 1, and for mode 2 (x faces) or 3 (y
       // faces) 1 on the low cell's face and -1 on the high cell's
       // (get_basis.f90): those products are exact and written out
@@ -153,14 +158,28 @@ __device__ __forceinline__ void face_point(const Consts& K, ML mL, MR mR, int g,
   Ez_out[g * fp + o] = ez;
 }
 
-template <int DIR>
+// GFAST: items run point-fastest (item = g + NG * face), so the five points
+// of a face sit on adjacent lanes and their loads of the two cells' modes
+// are served by the same cache lines; the face basis then comes from sb
+// (see face_point). Otherwise faces run fastest (item = face + nf * (g + NG
+// * row)) and every lane of a warp has the same g.
+template <int DIR, bool GFAST = false>
 __device__ __forceinline__ void face_item(const Consts& K, const double* __restrict__ U, double* __restrict__ Fh_out,
-                                          double* __restrict__ Ez_out, long long item) {
+                                          double* __restrict__ Ez_out, long long item,
+                                          const double* __restrict__ sb = nullptr) {
   const int nf = DIR == 0 ? K.nx + 1 : K.nx;
-  const int i0 = (int)(item % nf);
-  const long long r = item / nf;
-  const int g = (int)(r % NG);
-  const int j0 = (int)(r / NG);
+  int i0, g, j0;
+  if (GFAST) {
+    g = (int)(item % NG);
+    const long long f = item / NG;
+    i0 = (int)(f % nf);
+    j0 = (int)(f / nf);
+  } else {
+    i0 = (int)(item % nf);
+    const long long r = item / nf;
+    g = (int)(r % NG);
+    j0 = (int)(r / NG);
+  }
   long long cL, cR;
   if (DIR == 0) {
     cL = i0 + (long long)K.nx2 * (j0 + 1);
@@ -170,9 +189,9 @@ __device__ __forceinline__ void face_item(const Consts& K, const double* __restr
     cR = cL + K.nx2;
   }
   const long long pl = K.plane;
-  face_point<DIR>(
+  face_point<DIR, GFAST>(
       K, [&](int n, int d) { return U[pl * (d + 10 * n) + cL]; }, [&](int n, int d) { return U[pl * (d + 10 * n) + cR]; },
-      g, Fh_out, Ez_out, i0 + (long long)nf * j0);
+      g, Fh_out, Ez_out, i0 + (long long)nf * j0, sb);
 }
 
 // Faces of one block, staged: FACE_TILE faces of one face row at all NG
