@@ -1151,6 +1151,14 @@ __device__ __forceinline__ void char_limit_dir(const Consts& K, int dir, double 
 #ifndef GDF_TVB_STREAM
 #define GDF_TVB_STREAM 1
 #endif
+// the same for the characteristic limiter run inline by the one-pass
+// limiter (the learned gate, and the reference's all-cells limiter):
+// Orszag-Tang 512^2 (every cell limited) 3.64 against 3.67 ms per step, but
+// the learned blast 2048^2 45.9 against 45.6 ms and the learned blast 512^2
+// 5.70 against 5.68 (two A/B pairs, equal hashes), so it stays off
+#ifndef GDF_TVB_STREAM_INLINE
+#define GDF_TVB_STREAM_INLINE 0
+#endif
 
 template <bool ROLLED = false, bool STREAM = false>
 __device__ __forceinline__ void lim_tvb(const Consts& K, const double* __restrict__ S, long long c,
@@ -1356,7 +1364,7 @@ __device__ __forceinline__ void limit_item(const Consts& K, const double* __rest
   if (COMPACT) {
     if (lim_defer(gate, item, list, count)) return;
   } else if (gate) {
-    lim_tvb(K, S, c, m, word);
+    lim_tvb<false, GDF_TVB_STREAM_INLINE != 0>(K, S, c, m, word);
   }
   lim_finish(K, D, BX, BY, flags, stage, divfree, sc, item, i, j, c, m, word);
 }
