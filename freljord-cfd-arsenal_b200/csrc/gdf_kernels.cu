@@ -82,6 +82,11 @@
 #ifndef GDF_INFER_APART
 #define GDF_INFER_APART 1
 #endif
+// the learned gate's limiter in two passes as KXRCF's (gated cells listed,
+// then limited over full warps); 0: one pass
+#ifndef GDF_LEARNED_TWO_PASS
+#define GDF_LEARNED_TWO_PASS 1
+#endif
 
 
 namespace gdf {
@@ -738,12 +743,15 @@ static int launch_limit(GdfHandle* h, const double* S, double* D, int stage, con
       smem = LIMIT_SMEM_LEARNED;
     }
   }
-  // KXRCF: the gated cells go to a second pass over full warps (the sticky
-  // flags leave mixed warps for most of a run: the developed 512^2 rotor's
-  // limiter 1.8x faster). The learned gate stays in one pass: two passes
-  // measured slower there (blast 512^2, 82% gated: 8.16 against 7.50 ms per
-  // step), as for a plain run with nearly every cell gated (7.72 against 7.48).
-  const bool compact = K.detector == GDF_DETECT_KXRCF;
+  // KXRCF and the learned gate: the gated cells go to a second pass over
+  // full warps (the sticky flags leave mixed warps for most of a run: the
+  // developed 512^2 rotor's limiter 1.8x faster). For the learned gate the
+  // first pass then carries no characteristic limiter (496 B of stack
+  // against 896): learned blast 512^2, steps 1-1200, 5.41 against 5.67 ms
+  // per step; blast 2048^2 45.4 against 45.6 ms (same values). An earlier
+  // build had measured the two passes slower for the learned gate.
+  const bool compact = K.detector == GDF_DETECT_KXRCF ||
+                       (GDF_LEARNED_TWO_PASS && K.detector == GDF_DETECT_LEARNED && (GDF_INFER_APART || !infer));
   if (compact) CK(cudaMemsetAsync(h->lim_count, 0, sizeof(int32_t), h->st));
   int32_t *L = h->lim_list, *N = h->lim_count;
   int rc0 = run_kernel(h, GDF_K_LIMIT, [&] {
@@ -752,6 +760,10 @@ static int launch_limit(GdfHandle* h, const double* S, double* D, int stage, con
       k_limit<LIM_INFER, false><<<nb, LIM_BS, smem, h->st>>>(K, S, D, h->BX, h->BY, h->flags, h->trouble, stage,
                                                              fused_divfree, sc_gate, h->sc, h->net, h->QM, h->pnet,
                                                              h->t_lo, h->t_hi, nullptr, nullptr);
+    else if (K.detector == GDF_DETECT_LEARNED && compact)
+      k_limit<LIM_PNET, true><<<nb, LIM_BS, 0, h->st>>>(K, S, D, h->BX, h->BY, h->flags, h->trouble, stage,
+                                                        fused_divfree, sc_gate, h->sc, h->net, h->QM, h->pnet,
+                                                        h->t_lo, h->t_hi, L, N);
     else if (K.detector == GDF_DETECT_LEARNED)
       k_limit<LIM_PNET, false><<<nb, LIM_BS, 0, h->st>>>(K, S, D, h->BX, h->BY, h->flags, h->trouble, stage,
                                                          fused_divfree, sc_gate, h->sc, h->net, h->QM, h->pnet,
