@@ -85,7 +85,7 @@
 // the learned gate's limiter in two passes as KXRCF's (gated cells listed,
 // then limited over full warps); 0: one pass
 #ifndef GDF_LEARNED_TWO_PASS
-#define GDF_LEARNED_TWO_PASS 1
+#define GDF_LEARNED_TWO_PASS 0
 #endif
 
 
@@ -743,13 +743,14 @@ static int launch_limit(GdfHandle* h, const double* S, double* D, int stage, con
       smem = LIMIT_SMEM_LEARNED;
     }
   }
-  // KXRCF and the learned gate: the gated cells go to a second pass over
-  // full warps (the sticky flags leave mixed warps for most of a run: the
-  // developed 512^2 rotor's limiter 1.8x faster). For the learned gate the
-  // first pass then carries no characteristic limiter (496 B of stack
-  // against 896): learned blast 512^2, steps 1-1200, 5.41 against 5.67 ms
-  // per step; blast 2048^2 45.4 against 45.6 ms (same values). An earlier
-  // build had measured the two passes slower for the learned gate.
+  // KXRCF: the gated cells go to a second pass over full warps (the sticky
+  // flags leave mixed warps for most of a run: the developed 512^2 rotor's
+  // limiter 1.8x faster). The learned gate stays in one pass by default
+  // (GDF_LEARNED_TWO_PASS): two passes are faster while few cells are gated
+  // (learned blast 512^2, steps 1-1200, 5.41 against 5.67 ms per step;
+  // blast 2048^2 45.4 against 45.6 ms) but slower once most are (the whole
+  // 512^2 blast run to t = 0.01, 87% gated late: 7.86 against 7.13 ms per
+  // step), same values either way.
   const bool compact = K.detector == GDF_DETECT_KXRCF ||
                        (GDF_LEARNED_TWO_PASS && K.detector == GDF_DETECT_LEARNED && (GDF_INFER_APART || !infer));
   if (compact) CK(cudaMemsetAsync(h->lim_count, 0, sizeof(int32_t), h->st));
