@@ -750,7 +750,8 @@ static int launch_limit(GdfHandle* h, const double* S, double* D, int stage, con
   // (learned blast 512^2, steps 1-1200, 5.41 against 5.67 ms per step;
   // blast 2048^2 45.4 against 45.6 ms) but slower once most are (the whole
   // 512^2 blast run to t = 0.01, 87% gated late: 7.86 against 7.13 ms per
-  // step), same values either way.
+  // step, two bench runs whose plain steps took 7.15 and 7.14 ms), same
+  // values either way.
   const bool compact = K.detector == GDF_DETECT_KXRCF ||
                        (GDF_LEARNED_TWO_PASS && K.detector == GDF_DETECT_LEARNED && (GDF_INFER_APART || !infer));
   if (compact) CK(cudaMemsetAsync(h->lim_count, 0, sizeof(int32_t), h->st));
